@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""Benchmark of the FFT hot path on B200.
+
+Workload (the configuration the headline metric is quoted on): 3-D C2C FFT over all
+axes of a 256 x 256 x 256 complex64 array with a fused output fftshift and 1/N
+scaling transformation.  One step = one forward transform of one array resident in
+HBM; inputs are 134 MB each (larger than the 126 MB L2) and two input/output sets
+alternate between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl own|reference]
+
+Metric: algorithmic HBM throughput in GB/s, B_alg = P_min * (bytes_in + bytes_out)
+with P_min = ceil(log2(2^24) / log2(2^14)) = 2, i.e. 536,870,912 bytes per step.
+``e2e`` times the same call through the public API with pinned host buffers and the
+host<->device copies inside the timed region.  ``--impl reference`` times the CPU
+restatement of reikna's FFT (oracle/) on the host cores instead.
+Multi-GPU: one independent replica per GPU (no data-path collective; the transform
+does not need to shard), value = all replicas' bytes / max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+SHAPE = (256, 256, 256)
+NTOT = SHAPE[0] * SHAPE[1] * SHAPE[2]
+ELEM = 8
+ARRAY_BYTES = NTOT * ELEM
+P_MIN = 2
+B_ALG = P_MIN * 2 * ARRAY_BYTES
+FLOP = 5 * NTOT * math.log2(NTOT)
+METRIC = "C2C FFT GB/s vs HBM peak, plain vs batched/TC-split at stated err; serve p99 ms"
+CONFIG = {
+    "workload": "fft3d_256^3_complex64_fftshift_scale",
+    "shape": list(SHAPE),
+    "dtype": "complex64",
+    "axes": [0, 1, 2],
+    "transformations": ["fftshift (output)", "mul_const 1/N (output)"],
+    "bytes_per_step_algorithmic": B_ALG,
+    "l2": "inputs larger than L2 (134 MB each), two buffer sets alternate",
+}
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:  # noqa: BLE001
+            pass
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel_note: str):
+    """DRAM bytes per launch recorded by an ncu capture summary under profiles/."""
+    for f in sorted((ROOT / "profiles").glob("*.md")) + sorted((ROOT / "profiles").glob("*.txt")):
+        txt = f.read_text(errors="replace")
+        m = re.search(rf"traffic\[{re.escape(kernel_note)}\]\s*=\s*([0-9.eE+]+)", txt)
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL,
+                text=True,
+            )
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self) -> dict:
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": reasons,
+            "samples": len(rows),
+        }
+
+
+def cpu_baseline(x_host, seconds: float = 12.0) -> dict:
+    """The reikna-algorithm CPU oracle on this host, full workload per sample."""
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    plan = oracle.Plan(SHAPE, (0, 1, 2))
+    out = x_host.copy()
+    times = []
+    t_end = time.perf_counter() + seconds
+    while len(times) < 2 or (time.perf_counter() < t_end and len(times) < 50):
+        t0 = time.perf_counter()
+        plan.shifted(x_host, scale=1.0 / NTOT, threads=threads, out=out)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times[1:]) if len(times) > 2 else times[-1]
+    return {
+        "value": B_ALG / t / 1e9,
+        "unit": "GB/s",
+        "cores": threads,
+        "kind": "port",
+        "sample": f"full 256^3 complex64 FFT + fftshift + 1/N per sample, median of {len(times) - 1} after 1 warm-up",
+        "ms_per_step": t * 1e3,
+    }
+
+
+def run_reference(args, rank: int, world: int) -> int:
+    if rank != 0:
+        return 0
+    import numpy
+
+    from oracle import oracle
+
+    rng = numpy.random.default_rng(2)
+    x = (rng.standard_normal(SHAPE, numpy.float32) + 1j * rng.standard_normal(SHAPE, numpy.float32)).astype(numpy.complex64)
+    threads = os.cpu_count() or 1
+    plan = oracle.Plan(SHAPE, (0, 1, 2))
+    out = numpy.empty_like(x)
+    for _ in range(args.warmup):
+        plan.shifted(x, scale=1.0 / NTOT, threads=threads, out=out)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        plan.shifted(x, scale=1.0 / NTOT, threads=threads, out=out)
+    t = (time.perf_counter() - t0) / max(1, args.steps)
+    value = B_ALG / t / 1e9
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": CONFIG,
+        "cpu_baseline": {
+            "value": value,
+            "unit": "GB/s",
+            "cores": threads,
+            "kind": "port",
+            "sample": "full 256^3 complex64 FFT + fftshift + 1/N per step (C restatement of reikna's algorithm, OpenMP)",
+        },
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gflops": FLOP / t / 1e9,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_own(args, rank: int, world: int, local_rank: int) -> int:
+    import numpy
+    import torch
+
+    from reikna_b200 import transformations as tr
+    from reikna_b200.fft import FFT
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    gen = torch.Generator(device=dev).manual_seed(1234 + rank)
+    xs = [torch.complex(torch.randn(SHAPE, device=dev, generator=gen), torch.randn(SHAPE, device=dev, generator=gen)) for _ in range(2)]
+    outs = [torch.empty_like(xs[0]) for _ in range(2)]
+
+    fft = FFT(xs[0])
+    sh = tr.fftshift(xs[0])
+    sc = tr.mul_const(xs[0], 1.0 / NTOT)
+    fft.parameter.output.connect(sh, sh.input, shifted=sh.output)
+    fft.parameter.shifted.connect(sc, sc.input, result=sc.output)
+    comp = fft.compile(dev)
+    plan = comp._runner.plan
+    launches = plan.launches
+    passes = plan.describe()["passes"]
+
+    stream = torch.cuda.current_stream(dev)
+    for k in range(args.warmup):
+        comp(stream, outs[k % 2], xs[k % 2])
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    plan.profile(args.steps)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        barrier()
+        torch.cuda.synchronize(dev)
+        start.record(stream)
+        for k in range(args.steps):
+            comp(stream, outs[k % 2], xs[k % 2])
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+    ms = start.elapsed_time(end)
+    pass_ms, calls = plan.profile_read()
+    plan.profile(0)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * B_ALG * args.steps / (ms / 1e3) / 1e9
+
+    # end to end through the public API with pinned host buffers
+    h_in = xs[0].cpu().pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    d_in, d_out = torch.empty_like(xs[0]), torch.empty_like(xs[0])
+    e2e_steps = max(1, min(args.steps, 20))
+    for _ in range(2):
+        d_in.copy_(h_in, non_blocking=True)
+        comp(stream, d_out, d_in)
+        h_out.copy_(d_out, non_blocking=True)
+    torch.cuda.synchronize(dev)
+    barrier()
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(e2e_steps):
+        d_in.copy_(h_in, non_blocking=True)
+        comp(stream, d_out, d_in)
+        h_out.copy_(d_out, non_blocking=True)
+    e2.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = s2.elapsed_time(e2)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+        barrier()
+        dist.destroy_process_group()
+
+    if rank != 0:
+        return 0
+
+    # accuracy of the timed computation against the FP64 reference (outside timing)
+    x_host = xs[0].cpu().numpy()
+    y = h_out.numpy()
+    ref = numpy.fft.fftshift(numpy.fft.fftn(x_host.astype(numpy.complex128))) / NTOT
+    err = float(numpy.linalg.norm((y - ref).ravel()) / numpy.linalg.norm(ref.ravel()))
+
+    peak, peak_kind = peaks()
+    per_launch = [m / max(1, calls) for m in pass_ms]
+    dom = max(range(len(per_launch)), key=lambda i: per_launch[i])
+    dom_bytes = 2 * ARRAY_BYTES  # each pass reads and writes the whole array once
+    achieved = dom_bytes / (per_launch[dom] / 1e3) / 1e9
+    traffic = traffic_from_profiles(passes[dom]["note"] + f"/L{passes[dom]['L']}/{passes[dom]['mode']}")
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": dict(CONFIG, parallelism=f"replicas{world}"),
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "kernel": passes[dom]["note"] + f" L={passes[dom]['L']} {passes[dom]['mode']}",
+            "bytes_per_launch_algorithmic": dom_bytes,
+            "ms_per_launch": per_launch[dom],
+            "peak_kind": peak_kind,
+        },
+        "hbm_frac_step": (B_ALG / (ms / args.steps / 1e3) / 1e9) / peak,
+        "pass_ms": per_launch,
+        "passes": [f"{p['note']} L={p['L']} {p['mode']}" for p in passes],
+        "gflops": world * FLOP * args.steps / (ms / 1e3) / 1e9,
+        "rel_l2_vs_fp64": err,
+        "e2e": {
+            "value": world * B_ALG * e2e_steps / (ms_e2e / 1e3) / 1e9,
+            "unit": "GB/s",
+            "h2d_bytes_per_step": ARRAY_BYTES,
+            "d2h_bytes_per_step": ARRAY_BYTES,
+            "ms_per_step": ms_e2e / e2e_steps,
+        },
+        "gpu_launches": launches * args.steps,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(x_host)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["own", "reference"], default="own")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_own(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

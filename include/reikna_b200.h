@@ -1,0 +1,175 @@
+/*
+ * reikna_b200 -- C ABI of the B200 FFT library.
+ *
+ * This is the drop-in boundary for reikna's FFT hot path.  The Python classes in
+ * reikna_b200 (FFT, FFTShift, RFFT, Spectrogram) build an rk_fft_desc from the
+ * computation signature and its connected transformations and call these entry
+ * points through ctypes; any other host language can bind the same functions.
+ *
+ * All functions return RK_OK (0) on success or a negative RK_ERR_* code; the
+ * message of the last failure on the calling thread is returned by
+ * rk_last_error().  No C++ exception crosses this boundary.
+ *
+ * Reference interfaces replaced (file:line inside fjarri/reikna):
+ *   rk_fft_plan_create    FFT.__init__ (reikna/fft/fft.py:630) + Computation.compile
+ *                         (reikna/core/computation.py:259) + FFT._build_plan
+ *                         (reikna/fft/fft.py:723) + ComputationPlan.finalize
+ *                         (reikna/core/computation.py:642)
+ *   rk_fft_execute        ComputationCallable.__call__ (reikna/core/computation.py:766)
+ *   rk_fft_plan_destroy   Python GC of ComputationCallable / __tempalloc__
+ *                         (reikna/core/computation.py:764)
+ *   rk_fft_plan_describe  no runtime counterpart; exposes the kernel chain that
+ *                         get_fft_kernels (reikna/fft/fft.py:532) would build
+ *   rk_fftshift_execute   FFTShift compiled callable (reikna/fft/fftshift.py:65,
+ *                         reikna/fft/fftshift.mako:1-84)
+ */
+#ifndef REIKNA_B200_H
+#define REIKNA_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RK_API __attribute__((visibility("default")))
+#else
+#define RK_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RK_MAXD 8
+
+/* status codes */
+#define RK_OK 0
+#define RK_ERR_INVALID (-1)     /* bad descriptor or argument (reikna: ValueError) */
+#define RK_ERR_UNSUPPORTED (-2) /* valid request this build cannot plan */
+#define RK_ERR_CUDA (-3)        /* a CUDA runtime call failed */
+#define RK_ERR_NOMEM (-4)       /* device allocation failed */
+#define RK_ERR_DEVICE (-5)      /* device-side status word reported an error */
+
+/* element formats of edge arrays */
+#define RK_FMT_C64 1   /* complex64  (float2)  */
+#define RK_FMT_C128 2  /* complex128 (double2) */
+#define RK_FMT_F32 3   /* float32  real */
+#define RK_FMT_F64 4   /* float64  real */
+#define RK_FMT_F32_PAIR 5 /* two float32 arrays: real part, imaginary part */
+#define RK_FMT_F64_PAIR 6 /* two float64 arrays: real part, imaginary part */
+#define RK_FMT_I32 7   /* int32 (FFTShift only) */
+#define RK_FMT_C64_HALF 8 /* reserved */
+
+/* output post-operations (applied after scale) */
+#define RK_POST_NONE 0
+#define RK_POST_NORM 1 /* |z|^p, p = post_param; output format must be real (norm_const) */
+
+/* window applied on load along window_axis (spectrogram framing) */
+#define RK_WIN_NONE 0
+#define RK_WIN_HANN 1 /* 0.5*(1-cos(2*pi*p/(W-1))) for p < W, 1 beyond */
+
+/* plan flags */
+#define RK_FLAG_NO_PLANE 1   /* never fuse two axes into one clustered pass */
+#define RK_FLAG_NO_BLUE1 2   /* never use the single-pass Bluestein kernel */
+#define RK_FLAG_SPLIT_TC 4   /* tensor-core split-precision radix-16 stages */
+
+/*
+ * One side (input or output) of the FFT as the user sees it after the
+ * transformations are folded in.  Element (i_0, ..., i_{nd-1}) of the FFT array
+ * lives at   base + offset + sum_d ((i_d + shift_d) mod fft_shape_d) * strides_d
+ * (units: elements of the scalar format; complex elements for complex formats).
+ * An index with i_d >= shape_d is outside the user array: loads read 0 there
+ * (zero padding) and stores drop it (cropping).
+ */
+typedef struct rk_edge {
+    int32_t format;               /* RK_FMT_* */
+    int32_t ndim;                 /* must equal the FFT ndim */
+    int64_t shape[RK_MAXD];       /* extent of the user array along each FFT axis */
+    int64_t strides[RK_MAXD];     /* element strides */
+    int64_t offset;               /* first element offset, elements */
+    int64_t strides2[RK_MAXD];    /* strides of the imaginary array (PAIR formats) */
+    int64_t offset2;
+    int32_t shift[RK_MAXD];       /* index remap (fftshift); 0 = identity */
+    double scale_re, scale_im;    /* constant complex multiplier */
+    int32_t scale_slot;           /* runtime scalar multiplied in, -1 = none */
+    int32_t scale_div_slot;       /* runtime scalar divided by, -1 = none */
+    int32_t post;                 /* RK_POST_* (output side only) */
+    double post_param;
+    int32_t window;               /* RK_WIN_* (input side only) */
+    int32_t window_axis;
+    int64_t window_len;
+    int32_t conj;                 /* 1: conjugate the element (after scale) */
+} rk_edge;
+
+typedef struct rk_fft_desc {
+    int32_t dtype;                /* RK_FMT_C64 or RK_FMT_C128: compute precision */
+    int32_t ndim;
+    int64_t shape[RK_MAXD];       /* FFT array shape */
+    int32_t naxes;
+    int32_t axes[RK_MAXD];        /* transformed axes, any order, no repeats */
+    int32_t flags;                /* RK_FLAG_* */
+    rk_edge input;
+    rk_edge output;
+} rk_fft_desc;
+
+typedef struct rk_fft_plan rk_fft_plan;
+
+/* Initialise an edge to "contiguous array of the FFT shape, identity ops". */
+RK_API int rk_edge_init(rk_edge* e, int32_t format, int32_t ndim, const int64_t* shape);
+
+/* Build a plan on the current CUDA device: kernel chain, temporaries, twiddle and
+ * Bluestein tables (generated on the device in FP64).  Synchronous. */
+RK_API int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** plan);
+
+/* Run the plan asynchronously on `stream` (a cudaStream_t; NULL = legacy default).
+ * outputs/inputs: device pointers of the user arrays (2 for PAIR formats).
+ * inverse: 0 forward (exp(-i...)), 1 inverse normalised by 1/N (IFFT(FFT(x)) = x).
+ * scalars: n_scalars complex values, as (re, im) pairs of doubles, for the runtime
+ * scalar slots referenced by the edges.
+ * Output may alias input. */
+RK_API int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs,
+                   const void* const* inputs, int32_t n_inputs, int32_t inverse,
+                   const double* scalars, int32_t n_scalars, void* stream);
+
+RK_API int rk_fft_plan_destroy(rk_fft_plan* plan);
+
+/* Device bytes owned by the plan (temporaries + tables). */
+RK_API int rk_fft_plan_device_bytes(const rk_fft_plan* plan, int64_t* bytes);
+
+/* Describe the kernel chain as JSON text without touching the GPU (planner only).
+ * Writes at most `cap` bytes including the terminating NUL; *needed receives the
+ * full length. */
+RK_API int rk_fft_plan_describe(const rk_fft_desc* desc, char* buf, int64_t cap, int64_t* needed);
+
+/* Number of kernels rk_fft_execute launches for this plan. */
+RK_API int rk_fft_plan_launches(const rk_fft_plan* plan, int32_t* n);
+
+/* Per-pass timing: record a CUDA event pair around every kernel of the next
+ * `max_calls` rk_fft_execute calls (0 stops recording and frees the events).
+ * rk_fft_profile_read synchronises on the recorded events and returns, per pass,
+ * the summed milliseconds over the `*calls` recorded executions. */
+RK_API int rk_fft_profile(rk_fft_plan* plan, int32_t max_calls);
+RK_API int rk_fft_profile_read(rk_fft_plan* plan, double* ms_per_pass, int32_t n_passes, int32_t* calls);
+
+/*
+ * Standalone FFTShift (reikna/fft/fftshift.py:14): out = fftshift(in) over `axes`
+ * (inverse = 1: ifftshift).  Any element size in {4, 8, 16} bytes; contiguous
+ * C-order arrays.  Output may alias input (in-place swap kernel when every shifted
+ * axis is even, otherwise an out-of-place kernel through `scratch`, which must
+ * hold the whole array; scratch may be NULL when every axis is even).
+ */
+RK_API int rk_fftshift_execute(void* out, const void* in, int32_t elem_bytes, int32_t ndim,
+                        const int64_t* shape, int32_t naxes, const int32_t* axes,
+                        int32_t inverse, void* scratch, void* stream);
+
+RK_API const char* rk_last_error(void);
+
+/* Library version string. */
+RK_API const char* rk_version(void);
+
+/* sizeof(rk_edge) and sizeof(rk_fft_desc) as compiled, for binding checks. */
+RK_API int rk_abi_sizes(int64_t* edge_bytes, int64_t* desc_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* REIKNA_B200_H */

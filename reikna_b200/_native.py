@@ -1,0 +1,301 @@
+"""ctypes binding of the C ABI declared in ``include/reikna_b200.h``.
+
+The shared library is built in-tree by :mod:`reikna_b200.build`.  There is no CPU
+fallback: if the library cannot be loaded, every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import threading
+from pathlib import Path
+
+MAXD = 8
+
+OK = 0
+ERR_INVALID = -1
+ERR_UNSUPPORTED = -2
+ERR_CUDA = -3
+ERR_NOMEM = -4
+ERR_DEVICE = -5
+
+FMT_C64 = 1
+FMT_C128 = 2
+FMT_F32 = 3
+FMT_F64 = 4
+FMT_F32_PAIR = 5
+FMT_F64_PAIR = 6
+FMT_I32 = 7
+
+POST_NONE = 0
+POST_NORM = 1
+
+WIN_NONE = 0
+WIN_HANN = 1
+
+FLAG_NO_PLANE = 1
+FLAG_NO_BLUE1 = 2
+FLAG_SPLIT_TC = 4
+
+EXPORTED = (
+    "rk_edge_init",
+    "rk_fft_plan_create",
+    "rk_fft_execute",
+    "rk_fft_plan_destroy",
+    "rk_fft_plan_device_bytes",
+    "rk_fft_plan_describe",
+    "rk_fft_plan_launches",
+    "rk_fftshift_execute",
+    "rk_last_error",
+    "rk_version",
+    "rk_abi_sizes",
+    "rk_fft_profile",
+    "rk_fft_profile_read",
+)
+
+I64A = ctypes.c_int64 * MAXD
+I32A = ctypes.c_int32 * MAXD
+
+
+class Edge(ctypes.Structure):
+    _fields_ = [
+        ("format", ctypes.c_int32),
+        ("ndim", ctypes.c_int32),
+        ("shape", I64A),
+        ("strides", I64A),
+        ("offset", ctypes.c_int64),
+        ("strides2", I64A),
+        ("offset2", ctypes.c_int64),
+        ("shift", I32A),
+        ("scale_re", ctypes.c_double),
+        ("scale_im", ctypes.c_double),
+        ("scale_slot", ctypes.c_int32),
+        ("scale_div_slot", ctypes.c_int32),
+        ("post", ctypes.c_int32),
+        ("post_param", ctypes.c_double),
+        ("window", ctypes.c_int32),
+        ("window_axis", ctypes.c_int32),
+        ("window_len", ctypes.c_int64),
+        ("conj", ctypes.c_int32),
+    ]
+
+
+class FftDesc(ctypes.Structure):
+    _fields_ = [
+        ("dtype", ctypes.c_int32),
+        ("ndim", ctypes.c_int32),
+        ("shape", I64A),
+        ("naxes", ctypes.c_int32),
+        ("axes", I32A),
+        ("flags", ctypes.c_int32),
+        ("input", Edge),
+        ("output", Edge),
+    ]
+
+
+class NativeError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{message} (status {code})")
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def library_path() -> Path:
+    env = os.environ.get("REIKNA_B200_LIB")
+    if env:
+        return Path(env)
+    return Path(__file__).resolve().parent / "_lib" / "libreikna_b200.so"
+
+
+def lib() -> ctypes.CDLL:
+    """Load the shared library (once); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = library_path()
+        if not path.exists():
+            raise ImportError(
+                f"reikna_b200 native library not found at {path}; "
+                "build it with `python -m reikna_b200.build` (there is no CPU fallback)"
+            )
+        L = ctypes.CDLL(str(path))
+        vp = ctypes.c_void_p
+        L.rk_edge_init.argtypes = [ctypes.POINTER(Edge), ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
+        L.rk_fft_plan_create.argtypes = [ctypes.POINTER(FftDesc), ctypes.POINTER(vp)]
+        L.rk_fft_execute.argtypes = [
+            vp,
+            ctypes.POINTER(vp),
+            ctypes.c_int32,
+            ctypes.POINTER(vp),
+            ctypes.c_int32,
+            ctypes.c_int32,
+            ctypes.POINTER(ctypes.c_double),
+            ctypes.c_int32,
+            vp,
+        ]
+        L.rk_fft_plan_destroy.argtypes = [vp]
+        L.rk_fft_plan_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.rk_fft_plan_describe.argtypes = [
+            ctypes.POINTER(FftDesc),
+            ctypes.c_char_p,
+            ctypes.c_int64,
+            ctypes.POINTER(ctypes.c_int64),
+        ]
+        L.rk_fft_plan_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+        L.rk_fftshift_execute.argtypes = [
+            vp,
+            vp,
+            ctypes.c_int32,
+            ctypes.c_int32,
+            ctypes.POINTER(ctypes.c_int64),
+            ctypes.c_int32,
+            ctypes.POINTER(ctypes.c_int32),
+            ctypes.c_int32,
+            vp,
+            vp,
+        ]
+        L.rk_abi_sizes.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+        L.rk_fft_profile.argtypes = [vp, ctypes.c_int32]
+        L.rk_fft_profile_read.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+        L.rk_last_error.restype = ctypes.c_char_p
+        L.rk_version.restype = ctypes.c_char_p
+        for name in EXPORTED:
+            if name not in ("rk_last_error", "rk_version"):
+                getattr(L, name).restype = ctypes.c_int
+        eb, db = ctypes.c_int64(0), ctypes.c_int64(0)
+        L.rk_abi_sizes(ctypes.byref(eb), ctypes.byref(db))
+        if eb.value != ctypes.sizeof(Edge) or db.value != ctypes.sizeof(FftDesc):
+            raise ImportError(
+                f"ABI mismatch: C sizes edge={eb.value} desc={db.value}, "
+                f"ctypes sizes edge={ctypes.sizeof(Edge)} desc={ctypes.sizeof(FftDesc)}"
+            )
+        _lib = L
+        return L
+
+
+def check(code: int) -> None:
+    if code != OK:
+        msg = lib().rk_last_error().decode(errors="replace")
+        if code == ERR_INVALID:
+            raise ValueError(msg)
+        if code == ERR_UNSUPPORTED:
+            raise NotImplementedError(msg)
+        raise NativeError(code, msg)
+
+
+def edge(fmt: int, shape: tuple[int, ...]) -> Edge:
+    e = Edge()
+    arr = (ctypes.c_int64 * len(shape))(*shape)
+    check(lib().rk_edge_init(ctypes.byref(e), fmt, len(shape), arr))
+    return e
+
+
+def desc(dtype_fmt: int, shape: tuple[int, ...], axes: tuple[int, ...], flags: int = 0) -> FftDesc:
+    d = FftDesc()
+    d.dtype = dtype_fmt
+    d.ndim = len(shape)
+    for i, s in enumerate(shape):
+        d.shape[i] = s
+    d.naxes = len(axes)
+    for i, a in enumerate(axes):
+        d.axes[i] = a
+    d.flags = flags
+    d.input = edge(dtype_fmt, shape)
+    d.output = edge(dtype_fmt, shape)
+    return d
+
+
+def describe(d: FftDesc) -> dict:
+    """Planner output (kernel chain) as a dict; needs no GPU."""
+    need = ctypes.c_int64(0)
+    check(lib().rk_fft_plan_describe(ctypes.byref(d), None, 0, ctypes.byref(need)))
+    buf = ctypes.create_string_buffer(int(need.value))
+    check(lib().rk_fft_plan_describe(ctypes.byref(d), buf, need.value, ctypes.byref(need)))
+    return json.loads(buf.value.decode())
+
+
+class Plan:
+    """Owns an ``rk_fft_plan``; executes it on device pointers."""
+
+    def __init__(self, d: FftDesc):
+        self.desc = d
+        h = ctypes.c_void_p()
+        check(lib().rk_fft_plan_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        n = ctypes.c_int32(0)
+        check(lib().rk_fft_plan_launches(h, ctypes.byref(n)))
+        self.launches = int(n.value)
+
+    @property
+    def device_bytes(self) -> int:
+        b = ctypes.c_int64(0)
+        check(lib().rk_fft_plan_device_bytes(self._h, ctypes.byref(b)))
+        return int(b.value)
+
+    def execute(self, outs, ins, inverse: int = 0, scalars=(), stream: int = 0) -> None:
+        outs_a = (ctypes.c_void_p * len(outs))(*outs)
+        ins_a = (ctypes.c_void_p * len(ins))(*ins)
+        flat = []
+        for s in scalars:
+            c = complex(s)
+            flat += [c.real, c.imag]
+        sc = (ctypes.c_double * max(1, len(flat)))(*flat) if flat else None
+        check(
+            lib().rk_fft_execute(
+                self._h, outs_a, len(outs), ins_a, len(ins), int(inverse), sc, len(scalars), ctypes.c_void_p(stream)
+            )
+        )
+
+    def profile(self, max_calls: int) -> None:
+        """Record per-pass CUDA events for the next ``max_calls`` executions."""
+        check(lib().rk_fft_profile(self._h, int(max_calls)))
+
+    def profile_read(self) -> tuple[list[float], int]:
+        """(summed ms per pass, number of recorded executions); synchronises."""
+        ms = (ctypes.c_double * max(1, self.launches))()
+        calls = ctypes.c_int32(0)
+        check(lib().rk_fft_profile_read(self._h, ms, self.launches, ctypes.byref(calls)))
+        return list(ms[: self.launches]), int(calls.value)
+
+    def describe(self) -> dict:
+        return describe(self.desc)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().rk_fft_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+
+def fftshift_execute(out_ptr, in_ptr, elem_bytes, shape, axes, inverse, scratch_ptr, stream) -> None:
+    sh = (ctypes.c_int64 * len(shape))(*shape)
+    ax = (ctypes.c_int32 * max(1, len(axes)))(*axes)
+    check(
+        lib().rk_fftshift_execute(
+            ctypes.c_void_p(out_ptr),
+            ctypes.c_void_p(in_ptr),
+            elem_bytes,
+            len(shape),
+            sh,
+            len(axes),
+            ax,
+            int(inverse),
+            ctypes.c_void_p(scratch_ptr or 0),
+            ctypes.c_void_p(stream),
+        )
+    )

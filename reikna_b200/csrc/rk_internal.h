@@ -1,0 +1,87 @@
+// Host-side plan structures and kernel launch tables.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "rk_params.h"
+
+namespace rk {
+
+enum PassKind { PK_LINE = 0, PK_PLANE = 1 };
+enum BufId { BUF_IN = -1, BUF_OUT = -2 };
+
+using LineLaunch = cudaError_t (*)(const PassParams&, int64_t nblocks, cudaStream_t);
+using PlaneLaunch = cudaError_t (*)(const PlaneParams&, cudaStream_t);
+
+struct LineInfo {
+    LineLaunch fn;
+    int nt;        // threads per CTA
+    int nl;        // lines per CTA
+    size_t smem;   // dynamic shared memory bytes
+};
+
+struct PlaneInfo {
+    PlaneLaunch fn;
+    int q;         // cluster size
+    int nt;
+    size_t smem;
+};
+
+// lookup; returns false if the combination is not compiled
+bool line_info(int dbl, int L, int mode, int var, LineInfo* out);
+bool plane_info(int dbl, int L1, int L2, PlaneInfo* out);
+
+struct PassRec {
+    int kind = PK_LINE;
+    int dbl = 0;
+    int L = 0, mode = 0;
+    bool blue = false;
+    int L1 = 0, L2 = 0;            // plane
+    int axis = -1, axis2 = -1;
+    int ld_buf = BUF_IN, st_buf = BUF_OUT;
+    bool ld_edge = false, st_edge = false;
+    bool inplace_safe = true;      // each CTA rewrites only what it read
+    PassParams prm{};
+    PlaneParams pprm{};
+    int64_t nblocks = 0;
+    LineInfo li{};
+    PlaneInfo pi{};
+    std::string note;
+};
+
+struct DeviceTables {
+    void* tw_f = nullptr;      // float2[TWN]
+    void* tw_d = nullptr;      // double2[TWN]
+    void* tw4hi_f = nullptr;   // float2[4096]
+    void* tw4lo_f = nullptr;
+    void* tw4hi_d = nullptr;   // double2[4096]
+    void* tw4lo_d = nullptr;
+    int32_t* status = nullptr; // device status word
+};
+
+// per-device twiddle tables, generated once on the device in FP64
+int device_tables(int device, DeviceTables** out);
+
+void set_error(const std::string& msg);
+
+}  // namespace rk
+
+struct rk_fft_plan {
+    int device = 0;
+    rk_fft_desc desc{};
+    std::vector<rk::PassRec> passes;
+    std::vector<void*> temps;
+    std::vector<int64_t> temp_bytes;
+    std::vector<void*> tables;
+    int64_t device_bytes = 0;
+    double n_total = 1.0;          // inverse normalisation
+    bool alias_hazard = false;     // single remapping pass: in == out needs a copy
+    void* alias_tmp = nullptr;
+    int64_t in_extent_bytes = 0;   // bytes spanned by the input array (alias copy)
+    int64_t in2_extent_bytes = 0;
+    // per-pass event profiling (rk_fft_profile)
+    std::vector<cudaEvent_t> prof_ev;   // 2 * passes * max_calls
+    int32_t prof_max = 0, prof_used = 0;
+};

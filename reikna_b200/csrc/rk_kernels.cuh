@@ -1,0 +1,421 @@
+// Device side of the FFT passes.
+//
+// A pass transforms a tile of NL lines of length L held by one CTA.  The line FFT is
+// a Stockham autosort decomposition (natural-order output, no bit reversal): stage s
+// with radix R and P = product of the earlier radices takes, for butterfly b, the R
+// inputs at positions b + (L/R) m, applies an R-point register DFT, multiplies output
+// m' by W_{L/P}^{j1 m'} (j1 = b / P) and writes it to position (b % P) + P (m' + R j1).
+// The first stage reads HBM directly (positions are consecutive across threads, so
+// the loads coalesce) and the last stage writes HBM directly; only the stages in
+// between go through shared memory.  This is the role of reikna's fft_local /
+// fft_global passes (reikna/fft/fft.mako:750-1038), re-derived for sm_100a:
+// fixed compile-time radix plans, FP64-generated twiddle tables instead of per-element
+// sin/cos (reikna/fft/fft.mako:636-649), and transformations applied on the first
+// load and the last store (reikna/core/transformation_modules.py:260-318).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rk_dft.cuh"
+#include "rk_params.h"
+
+namespace rk {
+
+// ------------------------------------------------------------------------------
+// radix plans: RT elements per thread, NS stages with radices R[]
+// ------------------------------------------------------------------------------
+template <typename T, int L> struct Radix;
+#define RK_RADIX(TY, LL, RTV, ...)                                  \
+    template <> struct Radix<TY, LL> {                              \
+        static constexpr int RT = RTV;                              \
+        static constexpr int R[] = {__VA_ARGS__};                   \
+        static constexpr int NS = sizeof(R) / sizeof(int);          \
+    };
+RK_RADIX(float, 1, 1, 1)
+RK_RADIX(float, 2, 2, 2)
+RK_RADIX(float, 4, 4, 4)
+RK_RADIX(float, 8, 8, 8)
+RK_RADIX(float, 16, 16, 16)
+RK_RADIX(float, 32, 32, 32)
+RK_RADIX(float, 64, 8, 8, 8)
+RK_RADIX(float, 128, 16, 16, 8)
+RK_RADIX(float, 256, 16, 16, 16)
+RK_RADIX(float, 512, 32, 32, 16)
+RK_RADIX(float, 1024, 32, 32, 32)
+RK_RADIX(float, 2048, 16, 16, 16, 8)
+RK_RADIX(float, 4096, 16, 16, 16, 16)
+RK_RADIX(float, 8192, 32, 32, 16, 16)
+RK_RADIX(float, 16384, 32, 32, 32, 16)
+RK_RADIX(double, 1, 1, 1)
+RK_RADIX(double, 2, 2, 2)
+RK_RADIX(double, 4, 4, 4)
+RK_RADIX(double, 8, 8, 8)
+RK_RADIX(double, 16, 16, 16)
+RK_RADIX(double, 32, 8, 8, 4)
+RK_RADIX(double, 64, 8, 8, 8)
+RK_RADIX(double, 128, 16, 16, 8)
+RK_RADIX(double, 256, 16, 16, 16)
+RK_RADIX(double, 512, 8, 8, 8, 8)
+RK_RADIX(double, 1024, 16, 16, 16, 4)
+RK_RADIX(double, 2048, 16, 16, 16, 8)
+RK_RADIX(double, 4096, 16, 16, 16, 16)
+RK_RADIX(double, 8192, 16, 16, 16, 16, 2)
+#undef RK_RADIX
+
+template <typename T> struct Vec;   // lanes per 128-byte segment
+template <> struct Vec<float> { static constexpr int N = 16; };
+template <> struct Vec<double> { static constexpr int N = 8; };
+
+template <typename T, int L, int MODE> struct LineCfg {
+    using RC = Radix<T, L>;
+    static constexpr int RT = RC::RT;
+    static constexpr int TPL = L / RT;
+    static constexpr int ESZ = 2 * sizeof(T);
+    static constexpr int NL_POS = TPL >= 256 ? 1 : 256 / TPL;
+    static constexpr int NL_LANE_A = (256 / TPL) > Vec<T>::N ? (256 / TPL) : Vec<T>::N;
+    static constexpr int NL_LANE_B = 65536 / (L * ESZ);
+    static constexpr int NL_LANE = NL_LANE_A < NL_LANE_B ? NL_LANE_A : NL_LANE_B;
+    static constexpr int NL = MODE == MODE_POS ? NL_POS : NL_LANE;
+    static constexpr int NT = NL * TPL;
+    static constexpr int LS = L + L / 16;   // padded line stride (position mode)
+};
+
+// ------------------------------------------------------------------------------
+// integer helpers
+// ------------------------------------------------------------------------------
+__device__ __forceinline__ void divmod64(int64_t a, int64_t b, int64_t& q, int64_t& r) {
+    if (((uint64_t)a | (uint64_t)b) >> 32 == 0) {
+        uint32_t qa = (uint32_t)a / (uint32_t)b;
+        q = qa;
+        r = (uint32_t)a - qa * (uint32_t)b;
+    } else {
+        q = a / b;
+        r = a - q * b;
+    }
+}
+
+// flat element offset of a line on one side, plus validity
+struct LineAddr {
+    int64_t base;
+    int64_t c;
+    bool ok;
+};
+
+__device__ __forceinline__ int64_t dims_base(int nd, const int64_t* shape, const int64_t* stride,
+                                             const int64_t* bound, const int32_t* shift, int64_t idx,
+                                             bool& ok) {
+    int64_t base = 0;
+    for (int d = nd - 1; d >= 0; --d) {
+        int64_t q, r;
+        divmod64(idx, shape[d], q, r);
+        idx = q;
+        if (shift[d]) {
+            r += shift[d];
+            if (r >= shape[d]) r -= shape[d];
+        }
+        ok = ok && (r < bound[d]);
+        base += r * stride[d];
+    }
+    return base;
+}
+
+__device__ __forceinline__ LineAddr line_addr(const Side& s, int64_t line, int64_t C, int64_t I, bool lok) {
+    LineAddr la;
+    int64_t ci = C * I;
+    int64_t o, rem, c, i;
+    divmod64(line, ci, o, rem);
+    divmod64(rem, I, c, i);
+    bool ok = lok;
+    int64_t base = s.offset;
+    base += dims_base(s.nd_o, s.o_shape, s.o_stride, s.o_bound, s.o_shift, o, ok);
+    base += dims_base(s.nd_i, s.i_shape, s.i_stride, s.i_bound, s.i_shift, i, ok);
+    la.base = base;
+    la.c = c;
+    la.ok = ok;
+    return la;
+}
+
+// ------------------------------------------------------------------------------
+// element load / store with the fused value ops
+// ------------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ T hann(int64_t u, int32_t w) {
+    if (u >= w) return T(1);
+    // 0.5 * (1 - cos(2 pi u / (w - 1)))
+    T x = T(2) * T(u) / T(w - 1);
+    return T(0.5) * (T(1) - cospi(x));
+}
+
+template <typename T>
+__device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, int64_t j) {
+    using V = cplx<T>;
+    V v = cmk<V>(T(0), T(0));
+    const int64_t a = la.c * s.cA + j * s.jB;
+    if (la.ok && a < s.ax_len) {
+        int64_t u = a + s.ax_shift;
+        if (u >= s.ax_len) u -= s.ax_len;
+        if (u < s.ax_bound) {
+            const int64_t off = la.base + u * s.ax_stride;
+            switch (s.fmt) {
+                case RK_FMT_C64: {
+                    float2 t = reinterpret_cast<const float2*>(s.ptr)[off];
+                    v = cmk<V>((T)t.x, (T)t.y);
+                } break;
+                case RK_FMT_C128: {
+                    double2 t = reinterpret_cast<const double2*>(s.ptr)[off];
+                    v = cmk<V>((T)t.x, (T)t.y);
+                } break;
+                case RK_FMT_F32:
+                    v.x = (T)reinterpret_cast<const float*>(s.ptr)[off];
+                    break;
+                case RK_FMT_F64:
+                    v.x = (T)reinterpret_cast<const double*>(s.ptr)[off];
+                    break;
+                case RK_FMT_F32_PAIR:
+                    v.x = (T)reinterpret_cast<const float*>(s.ptr)[off];
+                    v.y = (T)reinterpret_cast<const float*>(s.ptr2)[off - s.offset + s.offset2];
+                    break;
+                case RK_FMT_F64_PAIR:
+                    v.x = (T)reinterpret_cast<const double*>(s.ptr)[off];
+                    v.y = (T)reinterpret_cast<const double*>(s.ptr2)[off - s.offset + s.offset2];
+                    break;
+                default:
+                    break;
+            }
+            if (s.flags & SF_WINDOW) v = cscale(v, hann<T>(u, s.win_len));
+        }
+    }
+    const int32_t f = s.flags;
+    if (f & SF_SCALE) v = cmul(v, cmk<V>((T)s.scale_re, (T)s.scale_im));
+    if (f & SF_PRE_CONJ) v = cconj(v);
+    // the tables hold ax_len entries; beyond that the element is the zero padding
+    if (a < s.ax_len) {
+        if (f & SF_CHIRP) v = cmul(v, reinterpret_cast<const V*>(s.chirp)[a]);
+        if (f & SF_TAB) v = cmul(v, reinterpret_cast<const V*>(s.tab)[a]);
+    }
+    if (f & SF_POST_CONJ) v = cconj(v);
+    return v;
+}
+
+// W_{tw4N}^(e) for e < tw4N via the two-level 2^24 table
+template <typename T>
+__device__ __forceinline__ cplx<T> tw4(const PassParams& p, int64_t e) {
+    using V = cplx<T>;
+    const int64_t k = (e & (p.tw4_N - 1)) * ((int64_t)1 << TW4_LOG) / p.tw4_N;
+    const V hi = reinterpret_cast<const V*>(p.tw4_hi)[k >> 12];
+    const V lo = reinterpret_cast<const V*>(p.tw4_lo)[k & (TW4_HALF - 1)];
+    return cmul(hi, lo);
+}
+
+template <typename T>
+__device__ __forceinline__ void side_store(const Side& s, const PassParams& p, const LineAddr& la, int64_t j,
+                                           cplx<T> v) {
+    using V = cplx<T>;
+    const int64_t a = la.c * s.cA + j * s.jB;
+    const int32_t f = s.flags;
+    if (f & SF_TW4) v = cmul(v, tw4<T>(p, la.c * j));
+    if (f & SF_PRE_CONJ) v = cconj(v);
+    if (!(la.ok && a < s.ax_len)) return;
+    if (f & SF_CHIRP) v = cmul(v, reinterpret_cast<const V*>(s.chirp)[a]);
+    if (f & SF_POST_CONJ) v = cconj(v);
+    if (f & SF_SCALE) v = cmul(v, cmk<V>((T)s.scale_re, (T)s.scale_im));
+    int64_t u = a + s.ax_shift;
+    if (u >= s.ax_len) u -= s.ax_len;
+    if (u >= s.ax_bound) return;
+    const int64_t off = la.base + u * s.ax_stride;
+    T nrm = T(0);
+    if (f & SF_NORM) {
+        nrm = v.x * v.x + v.y * v.y;
+        if (s.post_param != 2.0) nrm = pow(nrm, (T)(s.post_param * 0.5));
+    }
+    switch (s.fmt) {
+        case RK_FMT_C64:
+            reinterpret_cast<float2*>(s.ptr)[off] = make_float2((float)v.x, (float)v.y);
+            break;
+        case RK_FMT_C128:
+            reinterpret_cast<double2*>(s.ptr)[off] = make_double2((double)v.x, (double)v.y);
+            break;
+        case RK_FMT_F32:
+            reinterpret_cast<float*>(s.ptr)[off] = (float)((f & SF_NORM) ? nrm : v.x);
+            break;
+        case RK_FMT_F64:
+            reinterpret_cast<double*>(s.ptr)[off] = (double)((f & SF_NORM) ? nrm : v.x);
+            break;
+        case RK_FMT_F32_PAIR:
+            reinterpret_cast<float*>(s.ptr)[off] = (float)v.x;
+            reinterpret_cast<float*>(s.ptr2)[off - s.offset + s.offset2] = (float)v.y;
+            break;
+        case RK_FMT_F64_PAIR:
+            reinterpret_cast<double*>(s.ptr)[off] = (double)v.x;
+            reinterpret_cast<double*>(s.ptr2)[off - s.offset + s.offset2] = (double)v.y;
+            break;
+        default:
+            break;
+    }
+}
+
+// ------------------------------------------------------------------------------
+// Stockham engine
+// ------------------------------------------------------------------------------
+template <typename T, int L, int MODE> struct Engine {
+    using V = cplx<T>;
+    using Cfg = LineCfg<T, L, MODE>;
+    using RC = Radix<T, L>;
+    static constexpr int RT = Cfg::RT, TPL = Cfg::TPL, NL = Cfg::NL, NS = RC::NS;
+
+    static __device__ __forceinline__ int sidx(int ln, int pos) {
+        if constexpr (MODE == MODE_POS)
+            return ln * Cfg::LS + pos + (pos >> 4);
+        else
+            return pos * NL + ln;
+    }
+
+    // v[m] *= W_L^(e*m), m < R.  One table read gives w = W_L^e; w^2, w^3 and the
+    // powers w^(4q) (a product tree, at most 5 roundings deep for R = 32) give the
+    // rest as w^(4q) * w^r, so only R/4 + 3 complex values are live.
+    template <int R> static __device__ __forceinline__ void twiddle(V* v, int e, const V* tw) {
+        if constexpr (R > 1) {
+            const V w1 = tw[e * (TWN / L)];
+            v[1] = cmul(v[1], w1);
+            if constexpr (R > 2) {
+                const V w2 = cmul(w1, w1);
+                const V w3 = cmul(w2, w1);
+                v[2] = cmul(v[2], w2);
+                v[3] = cmul(v[3], w3);
+                if constexpr (R > 4) {
+                    constexpr int Q = R / 4;
+                    V wq[Q];
+                    wq[0] = cmk<V>(T(1), T(0));
+                    wq[1] = cmul(w2, w2);
+#pragma unroll
+                    for (int q = 2; q < Q; ++q) wq[q] = cmul(wq[q / 2], wq[q - q / 2]);
+#pragma unroll
+                    for (int q = 1; q < Q; ++q) {
+                        v[4 * q] = cmul(v[4 * q], wq[q]);
+                        v[4 * q + 1] = cmul(v[4 * q + 1], cmul(wq[q], w1));
+                        v[4 * q + 2] = cmul(v[4 * q + 2], cmul(wq[q], w2));
+                        v[4 * q + 3] = cmul(v[4 * q + 3], cmul(wq[q], w3));
+                    }
+                }
+            }
+        }
+    }
+
+    template <int S, int P>
+    static __device__ __forceinline__ void stages(V* v, V* sm, int ln, int tb, const V* tw) {
+        if constexpr (S < NS) {
+            constexpr int R = RC::R[S];
+            constexpr int NB = RT / R;
+#pragma unroll
+            for (int z = 0; z < NB; ++z) dft<R>(v + z * R);
+            if constexpr (S + 1 < NS) {
+#pragma unroll
+                for (int z = 0; z < NB; ++z) {
+                    const int b = tb + TPL * z;
+                    const int l = b % P, j1 = b / P;
+                    twiddle<R>(v + z * R, P * j1, tw);
+#pragma unroll
+                    for (int m = 0; m < R; ++m) sm[sidx(ln, l + P * (m + R * j1))] = v[z * R + m];
+                }
+                __syncthreads();
+                constexpr int R2 = RC::R[S + 1];
+                constexpr int NB2 = RT / R2;
+#pragma unroll
+                for (int z = 0; z < NB2; ++z)
+#pragma unroll
+                    for (int m = 0; m < R2; ++m) v[z * R2 + m] = sm[sidx(ln, tb + TPL * z + (L / R2) * m)];
+                __syncthreads();
+                stages<S + 1, P * R>(v, sm, ln, tb, tw);
+            }
+        }
+    }
+
+    // v holds stage-0 inputs: v[z*R0 + m] = x[tb + TPL z + (L/R0) m];
+    // afterwards v[z*Rl + m] = X[tb + TPL z + (L/Rl) m]
+    static __device__ __forceinline__ void run(V* v, V* sm, int ln, int tb, const V* tw) {
+        stages<0, 1>(v, sm, ln, tb, tw);
+    }
+
+    static constexpr int R0 = RC::R[0];
+    static constexpr int RL = RC::R[NS - 1];
+    static __device__ __forceinline__ int in_pos(int tb, int z, int m) { return tb + TPL * z + (L / R0) * m; }
+    static __device__ __forceinline__ int out_pos(int tb, int z, int m) { return tb + TPL * z + (L / RL) * m; }
+};
+
+// ------------------------------------------------------------------------------
+// line pass kernel (optionally a fused single-pass Bluestein convolution)
+// ------------------------------------------------------------------------------
+// VAR 0: plain pass; VAR 1: fused Bluestein convolution; VAR 2: position-mode
+// compute with a lane-fastest store through shared memory (four-step second pass,
+// whose output positions are strided by N1 while consecutive lines are adjacent).
+template <typename T, int L, int MODE, int VAR>
+__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassParams p) {
+    using V = cplx<T>;
+    using E = Engine<T, L, MODE>;
+    using Cfg = LineCfg<T, L, MODE>;
+    constexpr int RT = Cfg::RT, TPL = Cfg::TPL, NL = Cfg::NL;
+    constexpr int R0 = E::R0, RL = E::RL;
+    extern __shared__ __align__(16) unsigned char rk_smem[];
+    V* sm = reinterpret_cast<V*>(rk_smem);
+    const V* tw = reinterpret_cast<const V*>(p.tw);
+
+    const int tid = threadIdx.x;
+    const int ln = MODE == MODE_POS ? tid / TPL : tid % NL;
+    const int tb = MODE == MODE_POS ? tid % TPL : tid / NL;
+    const int64_t line = (int64_t)blockIdx.x * NL + ln;
+    const bool lok = line < p.nlines;
+
+    V v[RT];
+    {
+        const LineAddr la = line_addr(p.ld, line, p.C, p.I, lok);
+#pragma unroll
+        for (int z = 0; z < RT / R0; ++z)
+#pragma unroll
+            for (int m = 0; m < R0; ++m) v[z * R0 + m] = side_load<T>(p.ld, la, E::in_pos(tb, z, m));
+    }
+    E::run(v, sm, ln, tb, tw);
+    if constexpr (VAR == 1) {
+        // multiply by the kernel spectrum (1/M folded in) and conjugate, so that a
+        // second forward FFT followed by a conjugation yields the inverse FFT
+        const V* K = reinterpret_cast<const V*>(p.blue_k);
+#pragma unroll
+        for (int z = 0; z < RT / RL; ++z)
+#pragma unroll
+            for (int m = 0; m < RL; ++m) {
+                const int pos = E::out_pos(tb, z, m);
+                sm[E::sidx(ln, pos)] = cconj(cmul(v[z * RL + m], K[pos]));
+            }
+        __syncthreads();
+#pragma unroll
+        for (int z = 0; z < RT / R0; ++z)
+#pragma unroll
+            for (int m = 0; m < R0; ++m) v[z * R0 + m] = sm[E::sidx(ln, E::in_pos(tb, z, m))];
+        __syncthreads();
+        E::run(v, sm, ln, tb, tw);
+    }
+    if constexpr (VAR == 2) {
+        static_assert(MODE == MODE_POS, "transposed store needs position mode");
+#pragma unroll
+        for (int z = 0; z < RT / RL; ++z)
+#pragma unroll
+            for (int m = 0; m < RL; ++m) sm[E::sidx(ln, E::out_pos(tb, z, m))] = v[z * RL + m];
+        __syncthreads();
+        // thread t stores lane t % NL, positions t / NL + TPL * q
+        const int lane = tid % NL;
+        const int p0 = tid / NL;
+        const int64_t sline = (int64_t)blockIdx.x * NL + lane;
+        const LineAddr la = line_addr(p.st, sline, p.C, p.I, sline < p.nlines);
+#pragma unroll 4
+        for (int q = 0; q < RT; ++q) {
+            const int pos = p0 + TPL * q;
+            side_store<T>(p.st, p, la, pos, sm[E::sidx(lane, pos)]);
+        }
+    } else {
+        const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
+#pragma unroll
+        for (int z = 0; z < RT / RL; ++z)
+#pragma unroll
+            for (int m = 0; m < RL; ++m) side_store<T>(p.st, p, la, E::out_pos(tb, z, m), v[z * RL + m]);
+    }
+}
+
+}  // namespace rk

@@ -1,0 +1,987 @@
+// Host planner, device tables and C ABI of the FFT library.
+//
+// The planner follows the structure of reikna's get_fft_kernels
+// (reikna/fft/fft.py:532-584): axes are processed innermost first, a power-of-two
+// axis becomes a chain of passes, any other length goes through Bluestein's
+// algorithm at M = 2 * bounding_power_of_2(N) (reikna/fft/fft.py:551-561).  The pass
+// shapes are chosen for sm_100a instead of reikna's local/global split:
+//   * one pass per axis when the whole line (or a 128-byte-wide tile of strided
+//     lines) fits in one CTA's shared memory,
+//   * a two-pass four-step split (N = N1 * N2, twiddle W_N^(n2 k1) fused into the
+//     first pass' store) for longer axes (reikna uses radix-128 passes, fft.py:89),
+//   * Bluestein fused into a single pass (chirp, forward FFT, kernel spectrum,
+//     inverse FFT, chirp) when M fits one CTA, else four passes,
+//   * two adjacent axes of a plane fused into one clustered pass that exchanges
+//     rows and columns through distributed shared memory (rk_plane.cu).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "rk_internal.h"
+
+namespace rk {
+
+bool line_info_f32(int L, int mode, int var, LineInfo* out);
+bool line_info_f64(int L, int mode, int var, LineInfo* out);
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+
+bool line_info(int dbl, int L, int mode, int var, LineInfo* out) {
+    return dbl ? line_info_f64(L, mode, var, out) : line_info_f32(L, mode, var, out);
+}
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));               \
+            return e_ == cudaErrorMemoryAllocation ? RK_ERR_NOMEM : RK_ERR_CUDA;         \
+        }                                                                                \
+    } while (0)
+
+// ------------------------------------------------------------------------------
+// device tables (FP64 generation)
+// ------------------------------------------------------------------------------
+__global__ void k_gen_tables(float2* twf, double2* twd, float2* hif, float2* lof, double2* hid, double2* lod) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < TWN) {
+        double s, c;
+        // W_TWN^k = exp(-2 pi i k / TWN)
+        sincospi(2.0 * (double)k / (double)TWN, &s, &c);
+        twd[k] = make_double2(c, -s);
+        twf[k] = make_float2((float)c, (float)-s);
+    }
+    if (k < TW4_HALF) {
+        double s, c;
+        sincospi(2.0 * (double)k / (double)(1 << TW4_LOG), &s, &c);
+        lod[k] = make_double2(c, -s);
+        lof[k] = make_float2((float)c, (float)-s);
+        sincospi(2.0 * (double)k * TW4_HALF / (double)(1 << TW4_LOG), &s, &c);
+        hid[k] = make_double2(c, -s);
+        hif[k] = make_float2((float)c, (float)-s);
+    }
+}
+
+static std::mutex g_tab_mu;
+static std::map<int, DeviceTables*> g_tabs;
+
+int device_tables(int device, DeviceTables** out) {
+    std::lock_guard<std::mutex> lk(g_tab_mu);
+    auto it = g_tabs.find(device);
+    if (it != g_tabs.end()) {
+        *out = it->second;
+        return RK_OK;
+    }
+    DeviceTables* t = new DeviceTables();
+    CK(cudaMalloc(&t->tw_f, TWN * sizeof(float2)));
+    CK(cudaMalloc(&t->tw_d, TWN * sizeof(double2)));
+    CK(cudaMalloc(&t->tw4hi_f, TW4_HALF * sizeof(float2)));
+    CK(cudaMalloc(&t->tw4lo_f, TW4_HALF * sizeof(float2)));
+    CK(cudaMalloc(&t->tw4hi_d, TW4_HALF * sizeof(double2)));
+    CK(cudaMalloc(&t->tw4lo_d, TW4_HALF * sizeof(double2)));
+    CK(cudaMalloc(&t->status, sizeof(int32_t)));
+    CK(cudaMemset(t->status, 0, sizeof(int32_t)));
+    k_gen_tables<<<TWN / 256, 256>>>((float2*)t->tw_f, (double2*)t->tw_d, (float2*)t->tw4hi_f,
+                                      (float2*)t->tw4lo_f, (double2*)t->tw4hi_d, (double2*)t->tw4lo_d);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    g_tabs[device] = t;
+    *out = t;
+    return RK_OK;
+}
+
+// Bluestein tables.  chirp[k] = exp(-i pi (k^2 mod 2N) / N), k < N, with k^2 mod 2N
+// in exact 64-bit integers and the exponential in FP64.  b is the even sequence
+// conj(chirp) laid out on the padded length M exactly as reikna's get_kweights
+// (reikna/fft/fft.py:216-236): b[m] for m in [0, M-N], b[M-m] for m in [1, N-1].
+__global__ void k_gen_chirp(int64_t N, int64_t M, float2* cf, double2* cd, double2* b) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    const int64_t twoN = 2 * N;
+    auto chirp = [&](int64_t m) {
+        const int64_t r = (int64_t)(((unsigned __int128)m * (unsigned __int128)m) % (unsigned __int128)twoN);
+        double s, c;
+        sincospi((double)r / (double)N, &s, &c);
+        return make_double2(c, -s);
+    };
+    if (k < N) {
+        double2 c = chirp(k);
+        if (cd) cd[k] = c;
+        if (cf) cf[k] = make_float2((float)c.x, (float)c.y);
+    }
+    int64_t m;
+    if (k <= M - N)
+        m = k;
+    else
+        m = M - k;
+    double2 c = chirp(m);
+    b[k] = make_double2(c.x, -c.y);
+}
+
+__global__ void k_scale_convert(const double2* src, int64_t n, double s, float2* df, double2* dd) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double2 v = src[k];
+    v.x *= s;
+    v.y *= s;
+    if (dd) dd[k] = v;
+    if (df) df[k] = make_float2((float)v.x, (float)v.y);
+}
+
+// ------------------------------------------------------------------------------
+// planning
+// ------------------------------------------------------------------------------
+static bool is_pow2(int64_t n) { return n > 0 && (n & (n - 1)) == 0; }
+static int64_t bpow2(int64_t n) {
+    int64_t p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+static int ilog2(int64_t n) {
+    int l = 0;
+    while ((int64_t(1) << l) < n) ++l;
+    return l;
+}
+static int lane_max(int dbl) { return dbl ? 512 : 1024; }
+static int pos_max(int dbl) { return dbl ? 8192 : 16384; }
+static int fmt_is_complex(int f) { return f == RK_FMT_C64 || f == RK_FMT_C128; }
+static int fmt_is_pair(int f) { return f == RK_FMT_F32_PAIR || f == RK_FMT_F64_PAIR; }
+static int fmt_is_real(int f) { return f == RK_FMT_F32 || f == RK_FMT_F64; }
+
+// symbolic buffers while planning
+enum SymBuf { SB_IN = 0, SB_OUT = 1, SB_T0 = 2, SB_T1 = 3, SB_M0 = 4, SB_M1 = 5 };
+
+struct SideSpec {
+    int buf = SB_IN;
+    int64_t ax_len = 0;     // logical axis length seen through this buffer (N or M)
+    int64_t cA = 0, jB = 1;
+    int32_t flags = 0;
+    int chirp_axis = -1;    // Bluestein table owner (axis) for chirp
+    bool tab_k = false;     // kernel spectrum table
+};
+
+struct PassSpec {
+    int kind = PK_LINE;
+    int L = 0, mode = MODE_POS, var = 0;  // var: 0 plain, 1 Bluestein, 2 transposed store
+    int axis = -1, axis2 = -1;
+    int L1 = 0, L2 = 0;
+    int64_t O = 1, C = 1, I = 1;
+    bool inplace_safe = true;
+    int64_t tw4_N = 0;
+    int blue_axis = -1;     // fused Bluestein kernel spectrum owner
+    SideSpec ld, st;
+    std::string note;
+};
+
+struct BlueAxis {
+    int axis;
+    int64_t N, M;
+};
+
+struct Planned {
+    std::vector<PassSpec> passes;
+    std::vector<BlueAxis> blue;
+    bool need_T0 = false, need_T1 = false, need_M = false;
+    int64_t m_elems = 0;   // elements of an M-shaped temp
+};
+
+static int64_t prod_range(const int64_t* s, int a, int b) {
+    int64_t p = 1;
+    for (int i = a; i < b; ++i) p *= s[i];
+    return p;
+}
+
+static int plan_passes(const rk_fft_desc& d, Planned& P) {
+    const int dbl = d.dtype == RK_FMT_C128;
+    std::vector<int> axes(d.axes, d.axes + d.naxes);
+    std::sort(axes.begin(), axes.end(), std::greater<int>());
+    axes.erase(std::remove_if(axes.begin(), axes.end(), [&](int a) { return d.shape[a] == 1; }), axes.end());
+
+    const int nd = d.ndim;
+    int cur = SB_IN;
+    auto array_out = [&](bool inplace_ok) -> int {
+        if (inplace_ok && (cur == SB_T0 || cur == SB_T1)) return cur;
+        return cur == SB_T0 ? SB_T1 : SB_T0;
+    };
+
+    if (axes.empty()) {
+        // trivial problem: transformations still run (reikna/fft/fft.py:647-662).  One
+        // element per line: the last dim is the co-index c (a = c), L = 1.
+        PassSpec p;
+        p.L = 1;
+        p.axis = nd - 1;
+        p.O = prod_range(d.shape, 0, nd - 1);
+        p.C = d.shape[nd - 1];
+        p.I = 1;
+        p.ld.buf = SB_IN;
+        p.st.buf = SB_OUT;
+        p.ld.ax_len = p.st.ax_len = d.shape[nd - 1];
+        p.ld.cA = p.st.cA = 1;
+        p.ld.jB = p.st.jB = 0;
+        p.note = "copy";
+        P.passes.push_back(p);
+        return RK_OK;
+    }
+
+    const int LM = lane_max(dbl), PM = pos_max(dbl);
+    for (size_t ai = 0; ai < axes.size(); ++ai) {
+        const int ax = axes[ai];
+        const int64_t n = d.shape[ax];
+        const int64_t O = prod_range(d.shape, 0, ax);
+        const int64_t I = prod_range(d.shape, ax + 1, nd);
+        const bool last_axis = ai + 1 == axes.size();
+        if (n > (int64_t(1) << 30)) {
+            set_error("axis length too large");
+            return RK_ERR_UNSUPPORTED;
+        }
+        if (is_pow2(n)) {
+            if ((I == 1 && n <= PM) || (I > 1 && n <= LM)) {
+                PassSpec p;
+                p.L = (int)n;
+                p.mode = I == 1 ? MODE_POS : MODE_LANE;
+                p.axis = ax;
+                p.O = O; p.C = 1; p.I = I;
+                p.ld.buf = cur; p.ld.ax_len = n; p.ld.cA = 0; p.ld.jB = 1;
+                const int out = last_axis ? SB_OUT : array_out(true);
+                p.st.buf = out; p.st.ax_len = n; p.st.cA = 0; p.st.jB = 1;
+                p.note = "single";
+                P.passes.push_back(p);
+                cur = out;
+            } else {
+                // four-step n = N1 * N2: pass A over n1 (stride N2*I), pass B over n2
+                int64_t N1, N2;
+                if (I == 1) {
+                    N2 = std::min<int64_t>(256, n / 2);
+                    N1 = n / N2;
+                    if (N1 > LM) { N1 = LM; N2 = n / N1; }
+                    if (N2 > PM) {
+                        set_error("1-D length beyond two-pass range");
+                        return RK_ERR_UNSUPPORTED;
+                    }
+                } else {
+                    const int l = ilog2(n);
+                    N1 = int64_t(1) << (l / 2);
+                    N2 = n / N1;
+                    if (N1 > LM || N2 > LM) {
+                        set_error("strided axis length beyond two-pass range");
+                        return RK_ERR_UNSUPPORTED;
+                    }
+                }
+                PassSpec a;
+                a.L = (int)N1; a.mode = MODE_LANE; a.axis = ax;
+                a.O = O; a.C = N2; a.I = I;
+                a.ld.buf = cur; a.ld.ax_len = n; a.ld.cA = 1; a.ld.jB = N2;
+                const int mid = array_out(true);
+                a.st.buf = mid; a.st.ax_len = n; a.st.cA = 1; a.st.jB = N2;
+                a.st.flags |= SF_TW4; a.tw4_N = n;
+                a.note = "fourstep-A";
+                P.passes.push_back(a);
+                cur = mid;
+                PassSpec b;
+                b.L = (int)N2; b.axis = ax;
+                b.O = O; b.C = N1; b.I = I;
+                b.mode = I == 1 ? MODE_POS : MODE_LANE;
+                b.var = (I == 1 && N2 <= LM) ? 2 : 0;
+                b.inplace_safe = false;
+                b.ld.buf = cur; b.ld.ax_len = n; b.ld.cA = N2; b.ld.jB = 1;
+                const int out = last_axis ? SB_OUT : array_out(false);
+                b.st.buf = out; b.st.ax_len = n; b.st.cA = 1; b.st.jB = N1;
+                b.note = "fourstep-B";
+                P.passes.push_back(b);
+                cur = out;
+            }
+        } else {
+            const int64_t M = 2 * bpow2(n);
+            P.blue.push_back(BlueAxis{ax, n, M});
+            if ((I == 1 && M <= PM) || (I > 1 && M <= LM)) {
+                PassSpec p;
+                p.L = (int)M; p.var = 1; p.blue_axis = ax;
+                p.mode = I == 1 ? MODE_POS : MODE_LANE;
+                p.axis = ax;
+                p.O = O; p.C = 1; p.I = I;
+                p.ld.buf = cur; p.ld.ax_len = n; p.ld.cA = 0; p.ld.jB = 1;
+                p.ld.flags = SF_CHIRP; p.ld.chirp_axis = ax;
+                const int out = last_axis ? SB_OUT : array_out(true);
+                p.st.buf = out; p.st.ax_len = n; p.st.cA = 0; p.st.jB = 1;
+                p.st.flags = SF_PRE_CONJ | SF_CHIRP; p.st.chirp_axis = ax;
+                p.note = "bluestein-fused";
+                P.passes.push_back(p);
+                cur = out;
+            } else {
+                int64_t N1, N2;
+                if (I == 1) {
+                    N2 = std::min<int64_t>(256, M / 2);
+                    N1 = M / N2;
+                    if (N1 > LM) { N1 = LM; N2 = M / N1; }
+                    if (N2 > PM) {
+                        set_error("Bluestein length beyond two-pass range");
+                        return RK_ERR_UNSUPPORTED;
+                    }
+                } else {
+                    const int l = ilog2(M);
+                    N1 = int64_t(1) << (l / 2);
+                    N2 = M / N1;
+                    if (N1 > LM || N2 > LM) {
+                        set_error("strided Bluestein length beyond two-pass range");
+                        return RK_ERR_UNSUPPORTED;
+                    }
+                }
+                P.need_M = true;
+                P.m_elems = std::max<int64_t>(P.m_elems, O * M * I);
+                // forward FFT_M of chirp * x
+                PassSpec p1;
+                p1.L = (int)N1; p1.mode = MODE_LANE; p1.axis = ax; p1.O = O; p1.C = N2; p1.I = I;
+                p1.ld.buf = cur; p1.ld.ax_len = n; p1.ld.cA = 1; p1.ld.jB = N2;
+                p1.ld.flags = SF_CHIRP; p1.ld.chirp_axis = ax;
+                p1.st.buf = SB_M0; p1.st.ax_len = M; p1.st.cA = 1; p1.st.jB = N2;
+                p1.st.flags = SF_TW4; p1.tw4_N = M;
+                p1.note = "bluestein-A1";
+                PassSpec p2;
+                p2.L = (int)N2; p2.axis = ax; p2.O = O; p2.C = N1; p2.I = I;
+                p2.mode = I == 1 ? MODE_POS : MODE_LANE;
+                p2.var = (I == 1 && N2 <= LM) ? 2 : 0;
+                p2.inplace_safe = false;
+                p2.ld.buf = SB_M0; p2.ld.ax_len = M; p2.ld.cA = N2; p2.ld.jB = 1;
+                p2.st.buf = SB_M1; p2.st.ax_len = M; p2.st.cA = 1; p2.st.jB = N1;
+                p2.note = "bluestein-B1";
+                // inverse FFT_M of (spectrum * K) via conjugation
+                PassSpec p3 = p1;
+                p3.ld = SideSpec();
+                p3.ld.buf = SB_M1; p3.ld.ax_len = M; p3.ld.cA = 1; p3.ld.jB = N2;
+                p3.ld.flags = SF_TAB | SF_POST_CONJ; p3.ld.tab_k = true; p3.ld.chirp_axis = ax;
+                p3.st.buf = SB_M0;
+                p3.note = "bluestein-A2";
+                PassSpec p4 = p2;
+                p4.ld.buf = SB_M0;
+                const int out = last_axis ? SB_OUT : array_out(true);
+                p4.st = SideSpec();
+                p4.st.buf = out; p4.st.ax_len = n; p4.st.cA = 1; p4.st.jB = N1;
+                p4.st.flags = SF_PRE_CONJ | SF_CHIRP; p4.st.chirp_axis = ax;
+                p4.note = "bluestein-B2";
+                P.passes.push_back(p1);
+                P.passes.push_back(p2);
+                P.passes.push_back(p3);
+                P.passes.push_back(p4);
+                cur = out;
+            }
+        }
+    }
+    for (auto& p : P.passes) {
+        for (int b : {p.ld.buf, p.st.buf}) {
+            if (b == SB_T0) P.need_T0 = true;
+            if (b == SB_T1) P.need_T1 = true;
+        }
+    }
+    return RK_OK;
+}
+
+// ------------------------------------------------------------------------------
+// side construction
+// ------------------------------------------------------------------------------
+struct DimList {
+    int n = 0;
+    int64_t shape[MAXD], stride[MAXD], bound[MAXD];
+    int32_t shift[MAXD];
+    void push(int64_t sh, int64_t st, int64_t bd, int32_t sf) {
+        if (sh == 1) return;  // index is always 0
+        shape[n] = sh; stride[n] = st; bound[n] = bd; shift[n] = sf;
+        ++n;
+    }
+    void merge() {
+        // merge adjacent dims (row-major, last fastest) that form one contiguous range
+        int w = 0;
+        for (int i = 0; i < n; ++i) {
+            if (w > 0) {
+                int j = w - 1;
+                if (shift[j] == 0 && shift[i] == 0 && bound[j] == shape[j] && bound[i] == shape[i] &&
+                    stride[j] == stride[i] * shape[i]) {
+                    shape[j] *= shape[i];
+                    bound[j] = shape[j];
+                    stride[j] = stride[i];
+                    continue;
+                }
+            }
+            shape[w] = shape[i]; stride[w] = stride[i]; bound[w] = bound[i]; shift[w] = shift[i];
+            ++w;
+        }
+        n = w;
+    }
+};
+
+// Build the Side for buffer `buf` of a pass over axis `ax` of the FFT array.
+static void build_side(const rk_fft_desc& d, const SideSpec& ss, int ax, int dbl, bool is_load, Side& s) {
+    memset(&s, 0, sizeof(s));
+    const int nd = d.ndim;
+    const rk_edge* e = nullptr;
+    if (ss.buf == SB_IN) e = &d.input;
+    if (ss.buf == SB_OUT) e = &d.output;
+    int64_t shape[MAXD], stride[MAXD], bound[MAXD];
+    int32_t shift[MAXD];
+    for (int i = 0; i < nd; ++i) shape[i] = d.shape[i];
+    if (e) {
+        for (int i = 0; i < nd; ++i) {
+            stride[i] = e->strides[i];
+            bound[i] = std::min<int64_t>(e->shape[i], d.shape[i]);
+            shift[i] = e->shift[i];
+        }
+        s.fmt = e->format;
+        s.offset = e->offset;
+        s.offset2 = e->offset2;
+    } else {
+        // contiguous complex temp; the transformed axis may have the padded length
+        int64_t st = 1;
+        for (int i = nd - 1; i >= 0; --i) {
+            const int64_t len = (i == ax) ? ss.ax_len : shape[i];
+            stride[i] = st;
+            st *= len;
+            bound[i] = len;
+            shift[i] = 0;
+        }
+        s.fmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
+    }
+    DimList o, in;
+    for (int i = 0; i < ax; ++i) o.push(shape[i], stride[i], bound[i], shift[i]);
+    for (int i = ax + 1; i < nd; ++i) in.push(shape[i], stride[i], bound[i], shift[i]);
+    o.merge();
+    in.merge();
+    s.nd_o = o.n;
+    s.nd_i = in.n;
+    for (int i = 0; i < o.n; ++i) {
+        s.o_shape[i] = o.shape[i]; s.o_stride[i] = o.stride[i]; s.o_bound[i] = o.bound[i]; s.o_shift[i] = o.shift[i];
+    }
+    for (int i = 0; i < in.n; ++i) {
+        s.i_shape[i] = in.shape[i]; s.i_stride[i] = in.stride[i]; s.i_bound[i] = in.bound[i]; s.i_shift[i] = in.shift[i];
+    }
+    s.ax_len = ss.ax_len;
+    s.ax_bound = e ? std::min<int64_t>(bound[ax], ss.ax_len) : ss.ax_len;
+    s.ax_stride = stride[ax];
+    s.ax_shift = e ? shift[ax] : 0;
+    s.cA = ss.cA;
+    s.jB = ss.jB;
+    s.flags = ss.flags;
+    s.scale_re = 1.0;
+    s.scale_im = 0.0;
+    if (e) {
+        if (is_load && e->window != RK_WIN_NONE && e->window_axis == ax) {
+            s.flags |= SF_WINDOW;
+            s.win_len = (int32_t)e->window_len;
+        }
+        if (!is_load && e->post == RK_POST_NORM) {
+            s.flags |= SF_NORM;
+            s.post_param = e->post_param;
+        }
+    }
+}
+
+static int validate(const rk_fft_desc* d) {
+    if (!d) { set_error("null descriptor"); return RK_ERR_INVALID; }
+    if (d->dtype != RK_FMT_C64 && d->dtype != RK_FMT_C128) {
+        set_error("FFT computation requires array of a complex dtype");
+        return RK_ERR_INVALID;
+    }
+    if (d->ndim < 1 || d->ndim > RK_MAXD) { set_error("ndim out of range"); return RK_ERR_INVALID; }
+    for (int i = 0; i < d->ndim; ++i)
+        if (d->shape[i] < 1) { set_error("shape entries must be positive"); return RK_ERR_INVALID; }
+    if (d->naxes < 0 || d->naxes > d->ndim) { set_error("bad number of axes"); return RK_ERR_INVALID; }
+    bool seen[RK_MAXD] = {false};
+    for (int i = 0; i < d->naxes; ++i) {
+        int a = d->axes[i];
+        if (a < 0 || a >= d->ndim) { set_error("axis out of range"); return RK_ERR_INVALID; }
+        if (seen[a]) { set_error("repeated axis"); return RK_ERR_INVALID; }
+        seen[a] = true;
+    }
+    for (const rk_edge* e : {&d->input, &d->output}) {
+        if (e->ndim != d->ndim) { set_error("edge ndim must equal FFT ndim"); return RK_ERR_INVALID; }
+        for (int i = 0; i < d->ndim; ++i) {
+            if (e->shape[i] < 1) { set_error("edge shape entries must be positive"); return RK_ERR_INVALID; }
+            if (e->shift[i] < 0 || e->shift[i] >= d->shape[i]) {
+                set_error("edge shift out of range");
+                return RK_ERR_INVALID;
+            }
+        }
+        if (!(fmt_is_complex(e->format) || fmt_is_real(e->format) || fmt_is_pair(e->format))) {
+            set_error("unsupported edge format");
+            return RK_ERR_INVALID;
+        }
+    }
+    if (fmt_is_real(d->output.format) && d->output.post != RK_POST_NORM) {
+        set_error("real output requires a norm post-operation");
+        return RK_ERR_INVALID;
+    }
+    if (d->output.post == RK_POST_NORM && !fmt_is_real(d->output.format)) {
+        set_error("norm post-operation requires a real output format");
+        return RK_ERR_INVALID;
+    }
+    return RK_OK;
+}
+
+static const char* mode_name(int m) { return m == MODE_POS ? "pos" : "lane"; }
+static const char* buf_name(int b) {
+    switch (b) {
+        case SB_IN: return "input";
+        case SB_OUT: return "output";
+        case SB_T0: return "temp0";
+        case SB_T1: return "temp1";
+        case SB_M0: return "tempM0";
+        case SB_M1: return "tempM1";
+    }
+    return "?";
+}
+
+static std::string describe_json(const rk_fft_desc& d, const Planned& P) {
+    std::ostringstream os;
+    os << "{\"passes\": [";
+    for (size_t i = 0; i < P.passes.size(); ++i) {
+        const PassSpec& p = P.passes[i];
+        if (i) os << ", ";
+        os << "{\"kind\": \"" << (p.kind == PK_PLANE ? "plane" : "line") << "\", \"note\": \"" << p.note
+           << "\", \"axis\": " << p.axis << ", \"axis2\": " << p.axis2 << ", \"L\": " << p.L << ", \"L1\": " << p.L1
+           << ", \"L2\": " << p.L2 << ", \"mode\": \"" << mode_name(p.mode) << "\", \"var\": " << p.var
+           << ", \"O\": " << p.O << ", \"C\": " << p.C << ", \"I\": " << p.I << ", \"in\": \"" << buf_name(p.ld.buf)
+           << "\", \"out\": \"" << buf_name(p.st.buf) << "\"}";
+    }
+    os << "], \"bluestein\": [";
+    for (size_t i = 0; i < P.blue.size(); ++i) {
+        if (i) os << ", ";
+        os << "{\"axis\": " << P.blue[i].axis << ", \"N\": " << P.blue[i].N << ", \"M\": " << P.blue[i].M << "}";
+    }
+    os << "], \"temps\": {\"T0\": " << (P.need_T0 ? 1 : 0) << ", \"T1\": " << (P.need_T1 ? 1 : 0)
+       << ", \"M_elems\": " << P.m_elems << "}, \"dtype\": \"" << (d.dtype == RK_FMT_C128 ? "complex128" : "complex64")
+       << "\"}";
+    return os.str();
+}
+
+static int64_t edge_extent_bytes(const rk_edge& e, int second) {
+    int esz = 8;
+    switch (e.format) {
+        case RK_FMT_C64: esz = 8; break;
+        case RK_FMT_C128: esz = 16; break;
+        case RK_FMT_F32: case RK_FMT_F32_PAIR: esz = 4; break;
+        case RK_FMT_F64: case RK_FMT_F64_PAIR: esz = 8; break;
+    }
+    const int64_t* st = second ? e.strides2 : e.strides;
+    int64_t hi = second ? e.offset2 : e.offset, lo = hi;
+    for (int i = 0; i < e.ndim; ++i) {
+        const int64_t span = (e.shape[i] - 1) * st[i];
+        if (span > 0) hi += span; else lo += span;
+    }
+    return (hi + 1) * esz;
+}
+
+}  // namespace rk
+
+using namespace rk;
+
+// ------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------
+extern "C" {
+
+const char* rk_last_error(void) { return g_err.c_str(); }
+const char* rk_version(void) { return "reikna_b200 0.1.0 (sm_100a)"; }
+
+int rk_abi_sizes(int64_t* edge_bytes, int64_t* desc_bytes) {
+    if (!edge_bytes || !desc_bytes) {
+        set_error("null argument");
+        return RK_ERR_INVALID;
+    }
+    *edge_bytes = (int64_t)sizeof(rk_edge);
+    *desc_bytes = (int64_t)sizeof(rk_fft_desc);
+    return RK_OK;
+}
+
+int rk_edge_init(rk_edge* e, int32_t format, int32_t ndim, const int64_t* shape) {
+    if (!e || ndim < 1 || ndim > RK_MAXD || !shape) {
+        set_error("rk_edge_init: bad arguments");
+        return RK_ERR_INVALID;
+    }
+    memset(e, 0, sizeof(*e));
+    e->format = format;
+    e->ndim = ndim;
+    int64_t st = 1;
+    for (int i = ndim - 1; i >= 0; --i) {
+        e->shape[i] = shape[i];
+        e->strides[i] = st;
+        e->strides2[i] = st;
+        st *= shape[i];
+    }
+    e->scale_re = 1.0;
+    e->scale_im = 0.0;
+    e->scale_slot = -1;
+    e->scale_div_slot = -1;
+    e->post = RK_POST_NONE;
+    e->post_param = 2.0;
+    e->window = RK_WIN_NONE;
+    return RK_OK;
+}
+
+int rk_fft_plan_describe(const rk_fft_desc* desc, char* buf, int64_t cap, int64_t* needed) {
+    int rc = validate(desc);
+    if (rc) return rc;
+    Planned P;
+    rc = plan_passes(*desc, P);
+    if (rc) return rc;
+    std::string js = describe_json(*desc, P);
+    if (needed) *needed = (int64_t)js.size() + 1;
+    if (buf && cap > 0) {
+        const int64_t n = std::min<int64_t>(cap - 1, (int64_t)js.size());
+        memcpy(buf, js.data(), n);
+        buf[n] = 0;
+    }
+    return RK_OK;
+}
+
+int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
+    if (!out) { set_error("null plan pointer"); return RK_ERR_INVALID; }
+    *out = nullptr;
+    int rc = validate(desc);
+    if (rc) return rc;
+    Planned P;
+    rc = plan_passes(*desc, P);
+    if (rc) return rc;
+    const int dbl = desc->dtype == RK_FMT_C128;
+    const int esz = dbl ? 16 : 8;
+
+    // window must sit on the first processed axis
+    if (desc->input.window != RK_WIN_NONE && (P.passes.empty() || P.passes[0].axis != desc->input.window_axis)) {
+        set_error("window transformation must act along the first transformed axis");
+        return RK_ERR_UNSUPPORTED;
+    }
+
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    DeviceTables* tabs = nullptr;
+    rc = device_tables(dev, &tabs);
+    if (rc) return rc;
+
+    rk_fft_plan* plan = new rk_fft_plan();
+    plan->device = dev;
+    plan->desc = *desc;
+    auto fail = [&](int code) {
+        rk_fft_plan_destroy(plan);
+        return code;
+    };
+
+    // temporaries
+    int64_t arr_elems = 1;
+    for (int i = 0; i < desc->ndim; ++i) arr_elems *= desc->shape[i];
+    void* bufs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    auto alloc = [&](int64_t bytes, void** p) -> int {
+        cudaError_t e = cudaMalloc(p, (size_t)std::max<int64_t>(bytes, 16));
+        if (e != cudaSuccess) {
+            set_error(std::string("temporary allocation failed: ") + cudaGetErrorString(e));
+            return RK_ERR_NOMEM;
+        }
+        plan->temps.push_back(*p);
+        plan->temp_bytes.push_back(bytes);
+        plan->device_bytes += bytes;
+        return RK_OK;
+    };
+    if (P.need_T0 && (rc = alloc(arr_elems * esz, &bufs[SB_T0]))) return fail(rc);
+    if (P.need_T1 && (rc = alloc(arr_elems * esz, &bufs[SB_T1]))) return fail(rc);
+    if (P.need_M) {
+        if ((rc = alloc(P.m_elems * esz, &bufs[SB_M0]))) return fail(rc);
+        if ((rc = alloc(P.m_elems * esz, &bufs[SB_M1]))) return fail(rc);
+    }
+
+    // Bluestein tables: chirp (N) and kernel spectrum K = FFT_M(b) / M (M)
+    std::map<int, std::pair<void*, void*>> blue_tabs;
+    for (const BlueAxis& ba : P.blue) {
+        void *chirp = nullptr, *K = nullptr, *b = nullptr, *Kd = nullptr;
+        if ((rc = alloc(ba.N * esz, &chirp))) return fail(rc);
+        if ((rc = alloc(ba.M * esz, &K))) return fail(rc);
+        cudaError_t e1 = cudaMalloc(&b, ba.M * sizeof(double2));
+        cudaError_t e2 = cudaMalloc(&Kd, ba.M * sizeof(double2));
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            cudaFree(b); cudaFree(Kd);
+            set_error("Bluestein scratch allocation failed");
+            return fail(RK_ERR_NOMEM);
+        }
+        const int64_t nb = (ba.M + 255) / 256;
+        k_gen_chirp<<<(unsigned)nb, 256>>>(ba.N, ba.M, dbl ? nullptr : (float2*)chirp, dbl ? (double2*)chirp : nullptr,
+                                            (double2*)b);
+        cudaError_t ek = cudaGetLastError();
+        if (ek != cudaSuccess) {
+            cudaFree(b); cudaFree(Kd);
+            set_error(std::string("chirp generation failed: ") + cudaGetErrorString(ek));
+            return fail(RK_ERR_CUDA);
+        }
+        // forward FFT_M of b in complex128 with this library
+        rk_fft_desc kd;
+        memset(&kd, 0, sizeof(kd));
+        kd.dtype = RK_FMT_C128;
+        kd.ndim = 1;
+        kd.shape[0] = ba.M;
+        kd.naxes = 1;
+        kd.axes[0] = 0;
+        rk_edge_init(&kd.input, RK_FMT_C128, 1, kd.shape);
+        rk_edge_init(&kd.output, RK_FMT_C128, 1, kd.shape);
+        rk_fft_plan* kp = nullptr;
+        int krc = rk_fft_plan_create(&kd, &kp);
+        if (krc == RK_OK) {
+            void* o[1] = {Kd};
+            const void* in[1] = {b};
+            krc = rk_fft_execute(kp, o, 1, in, 1, 0, nullptr, 0, nullptr);
+        }
+        if (krc == RK_OK) {
+            k_scale_convert<<<(unsigned)nb, 256>>>((const double2*)Kd, ba.M, 1.0 / (double)ba.M,
+                                                   dbl ? nullptr : (float2*)K, dbl ? (double2*)K : nullptr);
+            cudaError_t e3 = cudaDeviceSynchronize();
+            if (e3 != cudaSuccess) {
+                set_error(std::string("Bluestein table generation failed: ") + cudaGetErrorString(e3));
+                krc = RK_ERR_CUDA;
+            }
+        }
+        if (kp) rk_fft_plan_destroy(kp);
+        cudaFree(b);
+        cudaFree(Kd);
+        if (krc != RK_OK) return fail(krc);
+        blue_tabs[ba.axis] = {chirp, K};
+    }
+
+    // materialise passes
+    int64_t ntot = 1;
+    for (int i = 0; i < desc->naxes; ++i) ntot *= desc->shape[desc->axes[i]];
+    plan->n_total = (double)ntot;
+    for (const PassSpec& ps : P.passes) {
+        PassRec r;
+        r.kind = ps.kind;
+        r.dbl = dbl;
+        r.L = ps.L;
+        r.mode = ps.mode;
+        r.blue = ps.var == 1;
+        r.axis = ps.axis;
+        r.ld_buf = ps.ld.buf == SB_IN ? BUF_IN : ps.ld.buf == SB_OUT ? BUF_OUT : ps.ld.buf;
+        r.st_buf = ps.st.buf == SB_IN ? BUF_IN : ps.st.buf == SB_OUT ? BUF_OUT : ps.st.buf;
+        r.ld_edge = ps.ld.buf == SB_IN;
+        r.st_edge = ps.st.buf == SB_OUT;
+        r.inplace_safe = ps.inplace_safe;
+        r.note = ps.note;
+        PassParams& pp = r.prm;
+        memset(&pp, 0, sizeof(pp));
+        pp.O = ps.O; pp.C = ps.C; pp.I = ps.I;
+        pp.nlines = ps.O * ps.C * ps.I;
+        build_side(*desc, ps.ld, ps.axis, dbl, true, pp.ld);
+        build_side(*desc, ps.st, ps.axis, dbl, false, pp.st);
+        if (!r.ld_edge) pp.ld.ptr = bufs[ps.ld.buf];
+        if (!r.st_edge) pp.st.ptr = bufs[ps.st.buf];
+        if (ps.ld.chirp_axis >= 0) {
+            auto& bt = blue_tabs[ps.ld.chirp_axis];
+            pp.ld.chirp = bt.first;
+            if (ps.ld.tab_k) pp.ld.tab = bt.second;
+        }
+        if (ps.st.chirp_axis >= 0) pp.st.chirp = blue_tabs[ps.st.chirp_axis].first;
+        if (ps.blue_axis >= 0) pp.blue_k = blue_tabs[ps.blue_axis].second;
+        pp.tw = dbl ? tabs->tw_d : tabs->tw_f;
+        pp.tw4_hi = dbl ? tabs->tw4hi_d : tabs->tw4hi_f;
+        pp.tw4_lo = dbl ? tabs->tw4lo_d : tabs->tw4lo_f;
+        pp.tw4_N = ps.tw4_N;
+        pp.status = tabs->status;
+        LineInfo li;
+        bool ok = line_info(dbl, ps.L, ps.mode, ps.var, &li);
+        if (!ok) {
+            set_error("no kernel instantiation for pass " + ps.note + " L=" + std::to_string(ps.L));
+            return fail(RK_ERR_UNSUPPORTED);
+        }
+        r.nblocks = (pp.nlines + li.nl - 1) / li.nl;
+        r.li = li;
+        plan->passes.push_back(r);
+    }
+    if (plan->passes.size() == 1) {
+        // a single pass rewrites only its own lines unless the two edges disagree
+        const Side& a = plan->passes[0].prm.ld;
+        const Side& b = plan->passes[0].prm.st;
+        bool same = a.fmt == b.fmt && a.nd_o == b.nd_o && a.nd_i == b.nd_i && a.ax_stride == b.ax_stride &&
+                    a.ax_shift == b.ax_shift && a.ax_bound == b.ax_bound && a.offset == b.offset;
+        for (int i = 0; same && i < a.nd_o; ++i)
+            same = a.o_stride[i] == b.o_stride[i] && a.o_shift[i] == b.o_shift[i] && a.o_shape[i] == b.o_shape[i] &&
+                   a.o_bound[i] == b.o_bound[i];
+        for (int i = 0; same && i < a.nd_i; ++i)
+            same = a.i_stride[i] == b.i_stride[i] && a.i_shift[i] == b.i_shift[i] && a.i_shape[i] == b.i_shape[i] &&
+                   a.i_bound[i] == b.i_bound[i];
+        plan->alias_hazard = !same || !plan->passes[0].inplace_safe;
+        plan->in_extent_bytes = edge_extent_bytes(desc->input, 0);
+        if (fmt_is_pair(desc->input.format)) plan->in2_extent_bytes = edge_extent_bytes(desc->input, 1);
+    }
+    // set launch attributes now (cudaFuncSetAttribute is not allowed during capture)
+    for (const PassRec& r : plan->passes) CK(r.li.fn(r.prm, 0, nullptr));
+    CK(cudaDeviceSynchronize());
+    *out = plan;
+    return RK_OK;
+}
+
+int rk_fft_profile(rk_fft_plan* plan, int32_t max_calls) {
+    if (!plan || max_calls < 0) { set_error("bad arguments"); return RK_ERR_INVALID; }
+    for (cudaEvent_t e : plan->prof_ev) cudaEventDestroy(e);
+    plan->prof_ev.clear();
+    plan->prof_max = plan->prof_used = 0;
+    if (max_calls == 0) return RK_OK;
+    const size_t n = 2 * plan->passes.size() * (size_t)max_calls;
+    plan->prof_ev.resize(n);
+    for (size_t i = 0; i < n; ++i) CK(cudaEventCreate(&plan->prof_ev[i]));
+    plan->prof_max = max_calls;
+    return RK_OK;
+}
+
+int rk_fft_profile_read(rk_fft_plan* plan, double* ms, int32_t n_passes, int32_t* calls) {
+    if (!plan || !ms || !calls || n_passes < (int32_t)plan->passes.size()) {
+        set_error("bad arguments");
+        return RK_ERR_INVALID;
+    }
+    const size_t np = plan->passes.size();
+    for (size_t p = 0; p < np; ++p) ms[p] = 0.0;
+    for (int32_t c = 0; c < plan->prof_used; ++c)
+        for (size_t p = 0; p < np; ++p) {
+            cudaEvent_t a = plan->prof_ev[2 * (c * np + p)], b = plan->prof_ev[2 * (c * np + p) + 1];
+            CK(cudaEventSynchronize(b));
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, a, b));
+            ms[p] += t;
+        }
+    *calls = plan->prof_used;
+    return RK_OK;
+}
+
+int rk_fft_plan_destroy(rk_fft_plan* plan) {
+    if (!plan) return RK_OK;
+    for (cudaEvent_t e : plan->prof_ev) cudaEventDestroy(e);
+    for (void* p : plan->temps) cudaFree(p);
+    if (plan->alias_tmp) cudaFree(plan->alias_tmp);
+    delete plan;
+    return RK_OK;
+}
+
+int rk_fft_plan_device_bytes(const rk_fft_plan* plan, int64_t* bytes) {
+    if (!plan || !bytes) { set_error("null argument"); return RK_ERR_INVALID; }
+    *bytes = plan->device_bytes;
+    return RK_OK;
+}
+
+int rk_fft_plan_launches(const rk_fft_plan* plan, int32_t* n) {
+    if (!plan || !n) { set_error("null argument"); return RK_ERR_INVALID; }
+    *n = (int32_t)plan->passes.size();
+    return RK_OK;
+}
+
+static void apply_edge_scale(const rk_edge& e, const double* scalars, int32_t n_scalars, double& re, double& im,
+                             int* bad) {
+    re = e.scale_re;
+    im = e.scale_im;
+    if (e.scale_slot >= 0) {
+        if (e.scale_slot >= n_scalars) { *bad = 1; return; }
+        const double sr = scalars[2 * e.scale_slot], si = scalars[2 * e.scale_slot + 1];
+        const double r = re * sr - im * si, i = re * si + im * sr;
+        re = r; im = i;
+    }
+    if (e.scale_div_slot >= 0) {
+        if (e.scale_div_slot >= n_scalars) { *bad = 1; return; }
+        const double sr = scalars[2 * e.scale_div_slot], si = scalars[2 * e.scale_div_slot + 1];
+        const double den = sr * sr + si * si;
+        const double r = (re * sr + im * si) / den, i = (im * sr - re * si) / den;
+        re = r; im = i;
+    }
+}
+
+int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
+                   int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars, void* stream) {
+    if (!plan) { set_error("null plan"); return RK_ERR_INVALID; }
+    const rk_fft_desc& d = plan->desc;
+    const int need_in = fmt_is_pair(d.input.format) ? 2 : 1;
+    const int need_out = fmt_is_pair(d.output.format) ? 2 : 1;
+    if (!inputs || !outputs || n_inputs < need_in || n_outputs < need_out) {
+        set_error("wrong number of input/output arrays");
+        return RK_ERR_INVALID;
+    }
+    for (int i = 0; i < need_in; ++i)
+        if (!inputs[i]) { set_error("null input pointer"); return RK_ERR_INVALID; }
+    for (int i = 0; i < need_out; ++i)
+        if (!outputs[i]) { set_error("null output pointer"); return RK_ERR_INVALID; }
+    cudaStream_t st = (cudaStream_t)stream;
+    const void* in0 = inputs[0];
+    const void* in1 = need_in > 1 ? inputs[1] : nullptr;
+
+    // in-place call of a single remapping pass: read from a private copy
+    if (plan->alias_hazard && (in0 == outputs[0] || (in1 && (in1 == outputs[0] || (need_out > 1 && in1 == outputs[1]))) ||
+                               (need_out > 1 && in0 == outputs[1]))) {
+        const int64_t need = plan->in_extent_bytes + plan->in2_extent_bytes + 256;
+        if (!plan->alias_tmp) {
+            cudaError_t e = cudaMalloc(&plan->alias_tmp, (size_t)need);
+            if (e != cudaSuccess) {
+                set_error("in-place staging allocation failed");
+                return RK_ERR_NOMEM;
+            }
+            plan->device_bytes += need;
+        }
+        char* t = (char*)plan->alias_tmp;
+        CK(cudaMemcpyAsync(t, in0, (size_t)plan->in_extent_bytes, cudaMemcpyDeviceToDevice, st));
+        in0 = t;
+        if (in1) {
+            char* t2 = t + ((plan->in_extent_bytes + 255) / 256) * 256;
+            CK(cudaMemcpyAsync(t2, in1, (size_t)plan->in2_extent_bytes, cudaMemcpyDeviceToDevice, st));
+            in1 = t2;
+        }
+    }
+
+    int bad = 0;
+    double in_re, in_im, out_re, out_im;
+    apply_edge_scale(d.input, scalars, n_scalars, in_re, in_im, &bad);
+    apply_edge_scale(d.output, scalars, n_scalars, out_re, out_im, &bad);
+    if (bad) { set_error("scalar slot out of range"); return RK_ERR_INVALID; }
+    if (inverse) {
+        out_re /= plan->n_total;
+        out_im /= plan->n_total;
+    }
+    const size_t np = plan->passes.size();
+    for (size_t i = 0; i < np; ++i) {
+        const PassRec& r = plan->passes[i];
+        PassParams p = r.prm;
+        if (r.ld_edge) {
+            p.ld.ptr = const_cast<void*>(in0);
+            p.ld.ptr2 = const_cast<void*>(in1);
+            if (in_re != 1.0 || in_im != 0.0) {
+                p.ld.flags |= SF_SCALE;
+                p.ld.scale_re = in_re;
+                p.ld.scale_im = in_im;
+            }
+            if (d.input.conj) p.ld.flags ^= SF_PRE_CONJ;
+        }
+        if (r.st_edge) {
+            p.st.ptr = outputs[0];
+            p.st.ptr2 = need_out > 1 ? outputs[1] : nullptr;
+            if (out_re != 1.0 || out_im != 0.0) {
+                p.st.flags |= SF_SCALE;
+                p.st.scale_re = out_re;
+                p.st.scale_im = out_im;
+            }
+        }
+        if (inverse) {
+            // IFFT(x) = conj(FFT(conj(x))) / N: conjugate on the first load and last store
+            if (i == 0) p.ld.flags ^= SF_PRE_CONJ;
+            if (i == np - 1) p.st.flags ^= SF_POST_CONJ;
+        }
+        if (r.st_edge && d.output.conj) p.st.flags ^= SF_POST_CONJ;
+        const bool prof = plan->prof_used < plan->prof_max;
+        const size_t ev = 2 * ((size_t)plan->prof_used * np + i);
+        if (prof) CK(cudaEventRecord(plan->prof_ev[ev], st));
+        cudaError_t e = r.li.fn(p, r.nblocks, st);
+        if (e != cudaSuccess) {
+            set_error(std::string("kernel launch failed (") + r.note + "): " + cudaGetErrorString(e));
+            return RK_ERR_CUDA;
+        }
+        if (prof) CK(cudaEventRecord(plan->prof_ev[ev + 1], st));
+    }
+    if (plan->prof_used < plan->prof_max) ++plan->prof_used;
+    return RK_OK;
+}
+
+}  // extern "C"

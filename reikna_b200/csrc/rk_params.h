@@ -1,0 +1,95 @@
+// Launch parameter blocks shared by the host planner and the device kernels.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/reikna_b200.h"
+
+namespace rk {
+
+constexpr int MAXD = RK_MAXD;
+
+// thread mapping of a line pass: position-fastest (lines contiguous along the FFT
+// axis) or lane-fastest (adjacent lines are adjacent in memory, strided axis)
+enum { MODE_POS = 0, MODE_LANE = 1 };
+
+// value-op flags of one pass side
+enum SideFlags : int32_t {
+    SF_PRE_CONJ = 1,    // conjugate first
+    SF_CHIRP = 2,       // multiply by chirp[a] (Bluestein)
+    SF_TAB = 4,         // multiply by tab[a]
+    SF_POST_CONJ = 8,   // conjugate after the tables
+    SF_SCALE = 16,      // multiply by (scale_re + i scale_im)
+    SF_WINDOW = 32,     // Hann window on the axis index (load side)
+    SF_NORM = 64,       // |z|^post_param (store side, real output)
+    SF_TW4 = 128,       // store side: multiply by W_tw4N^(c * k) (four-step twiddle)
+};
+
+// Addressing of one buffer in a pass.  A line l in [0, O*C*I) decomposes as
+// o = l / (C*I), c = (l / I) % C, i = l % I; o and i further decompose over the
+// outer / inner dims (row-major).  Element j of the line sits on the logical axis
+// index a = c*cA + j*jB; it is valid when a < ax_len and the user index
+// u = (a + ax_shift) mod ax_len is < ax_bound (likewise for every other dim).
+struct Side {
+    void* ptr;
+    void* ptr2;
+    int32_t fmt;
+    int32_t nd_o, nd_i;
+    int32_t flags;
+    int64_t o_shape[MAXD], o_stride[MAXD], o_bound[MAXD];
+    int64_t i_shape[MAXD], i_stride[MAXD], i_bound[MAXD];
+    int32_t o_shift[MAXD], i_shift[MAXD];
+    int64_t ax_len, ax_bound, ax_stride;
+    int64_t cA, jB;
+    int64_t offset, offset2;
+    int32_t ax_shift;
+    int32_t win_len;
+    double scale_re, scale_im;
+    double post_param;
+    const void* chirp;
+    const void* tab;
+};
+
+struct PassParams {
+    int64_t O, C, I;      // line decomposition
+    int64_t nlines;       // O*C*I
+    Side ld, st;
+    const void* tw;       // W_TWN^k, k < TWN (precision of the pass)
+    const void* tw4_hi;   // W_2^24^(4096 k)
+    const void* tw4_lo;   // W_2^24^k
+    int64_t tw4_N;        // four-step twiddle modulus (power of two <= 2^24)
+    const void* blue_k;   // Bluestein kernel spectrum (fused single-pass kernel)
+    int32_t* status;
+};
+
+// Clustered two-axis pass: axis r (rows, length L1) and the contiguous axis q
+// (columns, length L2) of a plane; the plane index o decomposes over outer dims.
+struct PlaneSide {
+    void* ptr;
+    void* ptr2;
+    int32_t fmt;
+    int32_t nd_o;
+    int32_t flags;
+    int32_t win_len;
+    int64_t o_shape[MAXD], o_stride[MAXD], o_bound[MAXD];
+    int32_t o_shift[MAXD];
+    int64_t r_len, r_bound, r_stride;
+    int64_t q_len, q_bound, q_stride;
+    int32_t r_shift, q_shift;
+    int64_t offset, offset2;
+    double scale_re, scale_im;
+    double post_param;
+};
+
+struct PlaneParams {
+    int64_t nplanes;
+    PlaneSide ld, st;
+    const void* tw;
+    int32_t* status;
+};
+
+constexpr int TWN_LOG = 14;           // base twiddle table: W_16384^k
+constexpr int TWN = 1 << TWN_LOG;
+constexpr int TW4_LOG = 24;           // two-level table for four-step twiddles
+constexpr int TW4_HALF = 4096;
+
+}  // namespace rk

@@ -1,0 +1,92 @@
+"""``FFT`` computation: drop-in for ``reikna.fft.FFT`` (reikna/fft/fft.py:595-756).
+
+Same constructor ``FFT(arr_t, axes=None)``, same signature
+``(output:o, input:i, inverse:s int32 = 0)``, same semantics: the forward transform
+uses exp(-2 pi i n k / N), the inverse is normalised so that IFFT(FFT(x)) = x, output
+may alias input, transformations connected to ``input``/``output`` run inside the
+first and last pass.  Planning and the kernels are native (``include/reikna_b200.h``).
+"""
+
+from __future__ import annotations
+
+import numpy
+
+from .. import _native as N
+from ..core.computation import Computation, array_pointer, scalar_value
+from ..core.signature import Annotation, ArrayMetadata, Parameter, Type
+from ._fold import edge_struct, fold_input, fold_output
+
+
+def _is_complex(dtype) -> bool:
+    return numpy.dtype(dtype).kind == "c"
+
+
+class FFT(Computation):
+    """Fast Fourier Transform over ``axes`` of an array of ``arr_t``'s type.
+
+    :param arr_t: array-like (torch tensor, numpy array, ``ArrayMetadata``, ``Type``).
+    :param axes: axes to transform (default: all); negative values count from the end.
+    """
+
+    def __init__(self, arr_t, axes=None):
+        meta = Type(arr_t).as_array_metadata() if not isinstance(arr_t, ArrayMetadata) else arr_t
+        if not _is_complex(meta.dtype):
+            raise ValueError("FFT computation requires array of a complex dtype")
+        Computation.__init__(
+            self,
+            [
+                Parameter("output", Annotation(meta, "o")),
+                Parameter("input", Annotation(meta, "i")),
+                Parameter("inverse", Annotation(numpy.int32), default=0),
+            ],
+        )
+        nd = len(meta.shape)
+        axes = tuple(range(nd)) if axes is None else tuple(int(a) for a in axes)
+        axes = tuple(a + nd if a < 0 else a for a in axes)
+        if any(a < 0 or a >= nd for a in axes) or len(set(axes)) != len(axes):
+            raise ValueError(f"invalid axes {axes} for a {nd}-dimensional array")
+        self._axes = axes
+        self._meta = meta
+
+    def native_descriptor(self, flags: int = 0):
+        """The ``rk_fft_desc`` this computation compiles to, and its argument layout."""
+        meta = self._meta
+        tree = self._tr_tree
+        shape = tuple(meta.shape)
+        ispec = fold_input(tree, "input", shape)
+        ospec = fold_output(tree, "output", shape)
+        leaves = tree.get_leaf_parameters()
+        scalar_names = [p.name for p in leaves if p.annotation.is_scalar() and p.name != "inverse"]
+        slots = {name: i for i, name in enumerate(scalar_names)}
+        d = N.FftDesc()
+        d.dtype = N.FMT_C64 if meta.dtype == numpy.complex64 else N.FMT_C128
+        d.ndim = len(shape)
+        for i, s in enumerate(shape):
+            d.shape[i] = s
+        d.naxes = len(self._axes)
+        for i, a in enumerate(self._axes):
+            d.axes[i] = a
+        d.flags = flags
+        d.input = edge_struct(ispec, slots)
+        d.output = edge_struct(ospec, slots)
+        return d, ispec, ospec, scalar_names
+
+    def describe(self, flags: int = 0) -> dict:
+        """Kernel chain the native planner builds for this computation (no GPU needed)."""
+        d, *_ = self.native_descriptor(flags)
+        return N.describe(d)
+
+    def _build_runner(self, device, flags: int = 0, **_ignored):
+        d, ispec, ospec, scalar_names = self.native_descriptor(flags)
+        plan = N.Plan(d)
+        ann = {p.name: p.annotation for p in self._tr_tree.get_leaf_parameters()}
+
+        def runner(stream: int, args):
+            outs = [array_pointer(args[n], ann[n]) for n in ospec.arrays]
+            ins = [array_pointer(args[n], ann[n]) for n in ispec.arrays]
+            scalars = [scalar_value(args[n]) for n in scalar_names]
+            plan.execute(outs, ins, inverse=int(args["inverse"]), scalars=scalars, stream=stream)
+
+        runner.launches = plan.launches
+        runner.plan = plan
+        return runner

@@ -1,0 +1,47 @@
+import os
+import sys
+from pathlib import Path
+
+import numpy
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    config.addinivalue_line("markers", "slow: long-running case")
+
+
+def _cuda_available() -> bool:
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:  # noqa: BLE001
+        return False
+
+
+def pytest_collection_modifyitems(config, items):
+    if _cuda_available():
+        return
+    skip = pytest.mark.skip(reason="no CUDA device in this environment")
+    for item in items:
+        if "gpu" in item.keywords:
+            item.add_marker(skip)
+
+
+@pytest.fixture
+def rng(request):
+    # seeded per test for reproducibility
+    seed = abs(hash(request.node.nodeid)) % (2**32)
+    return numpy.random.default_rng(seed)
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    import torch
+
+    return torch.device("cuda", 0)
