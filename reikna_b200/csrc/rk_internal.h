@@ -13,7 +13,7 @@ enum PassKind { PK_LINE = 0, PK_PLANE = 1 };
 enum BufId { BUF_IN = -1, BUF_OUT = -2 };
 
 using LineLaunch = cudaError_t (*)(const PassParams&, int64_t nblocks, cudaStream_t);
-using PlaneLaunch = cudaError_t (*)(const PlaneParams&, cudaStream_t);
+using PlaneLaunch = cudaError_t (*)(const PassParams&, int64_t nplanes, cudaStream_t);
 
 struct LineInfo {
     LineLaunch fn;
@@ -52,8 +52,11 @@ struct PassRec {
 };
 
 struct DeviceTables {
-    void* tw_f = nullptr;      // float2[TWN]
-    void* tw_d = nullptr;      // double2[TWN]
+    void* stw_f = nullptr;     // float2 stage twiddle tables, all L (TwLayout)
+    void* stw_d = nullptr;     // double2 stage twiddle tables
+    int64_t off_f[16] = {0};   // element offset of the table of L = 2^i
+    int64_t off_d[16] = {0};
+    int64_t bytes = 0;
     void* tw4hi_f = nullptr;   // float2[4096]
     void* tw4lo_f = nullptr;
     void* tw4hi_d = nullptr;   // double2[4096]

@@ -62,6 +62,25 @@ RK_RADIX(double, 4096, 16, 16, 16, 16)
 RK_RADIX(double, 8192, 16, 16, 16, 16, 2)
 #undef RK_RADIX
 
+// Stage twiddle tables of a length-L line: stage s (radix R, P = product of the
+// earlier radices, J = L / (P R) butterfly groups) needs W_{L/P}^(j1 m) for
+// 1 <= m < R, j1 < J, stored as [m - 1][j1]; the stages follow each other and the
+// last stage needs none.  Generated in FP64 on the device (rk_lib.cu).
+template <typename T, int L> struct TwLayout {
+    using RC = Radix<T, L>;
+    static constexpr int size_of(int s) {
+        int P = 1;
+        for (int i = 0; i < s; ++i) P *= RC::R[i];
+        return (RC::R[s] - 1) * (L / (P * RC::R[s]));
+    }
+    static constexpr int offset(int s) {
+        int o = 0;
+        for (int i = 0; i < s; ++i) o += size_of(i);
+        return o;
+    }
+    static constexpr int total() { return RC::NS > 1 ? offset(RC::NS - 1) : 0; }
+};
+
 template <typename T> struct Vec;   // lanes per 128-byte segment
 template <> struct Vec<float> { static constexpr int N = 16; };
 template <> struct Vec<double> { static constexpr int N = 8; };
@@ -256,11 +275,11 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
 // ------------------------------------------------------------------------------
 // Stockham engine
 // ------------------------------------------------------------------------------
-template <typename T, int L, int MODE> struct Engine {
+template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct Engine {
     using V = cplx<T>;
     using Cfg = LineCfg<T, L, MODE>;
     using RC = Radix<T, L>;
-    static constexpr int RT = Cfg::RT, TPL = Cfg::TPL, NL = Cfg::NL, NS = RC::NS;
+    static constexpr int RT = Cfg::RT, TPL = Cfg::TPL, NL = NL_, NS = RC::NS;
 
     static __device__ __forceinline__ int sidx(int ln, int pos) {
         if constexpr (MODE == MODE_POS)
@@ -269,35 +288,11 @@ template <typename T, int L, int MODE> struct Engine {
             return pos * NL + ln;
     }
 
-    // v[m] *= W_L^(e*m), m < R.  One table read gives w = W_L^e; w^2, w^3 and the
-    // powers w^(4q) (a product tree, at most 5 roundings deep for R = 32) give the
-    // rest as w^(4q) * w^r, so only R/4 + 3 complex values are live.
-    template <int R> static __device__ __forceinline__ void twiddle(V* v, int e, const V* tw) {
-        if constexpr (R > 1) {
-            const V w1 = tw[e * (TWN / L)];
-            v[1] = cmul(v[1], w1);
-            if constexpr (R > 2) {
-                const V w2 = cmul(w1, w1);
-                const V w3 = cmul(w2, w1);
-                v[2] = cmul(v[2], w2);
-                v[3] = cmul(v[3], w3);
-                if constexpr (R > 4) {
-                    constexpr int Q = R / 4;
-                    V wq[Q];
-                    wq[0] = cmk<V>(T(1), T(0));
-                    wq[1] = cmul(w2, w2);
+    // v[m] *= W_{L/P}^(j1 m), 1 <= m < R, read from the stage table laid out
+    // [m - 1][j1] (TwLayout): every factor is an FP64 value rounded once.
+    template <int R, int J> static __device__ __forceinline__ void twiddle(V* v, int j1, const V* tws) {
 #pragma unroll
-                    for (int q = 2; q < Q; ++q) wq[q] = cmul(wq[q / 2], wq[q - q / 2]);
-#pragma unroll
-                    for (int q = 1; q < Q; ++q) {
-                        v[4 * q] = cmul(v[4 * q], wq[q]);
-                        v[4 * q + 1] = cmul(v[4 * q + 1], cmul(wq[q], w1));
-                        v[4 * q + 2] = cmul(v[4 * q + 2], cmul(wq[q], w2));
-                        v[4 * q + 3] = cmul(v[4 * q + 3], cmul(wq[q], w3));
-                    }
-                }
-            }
-        }
+        for (int m = 1; m < R; ++m) v[m] = cmul(v[m], __ldg(tws + (m - 1) * J + j1));
     }
 
     template <int S, int P>
@@ -308,11 +303,13 @@ template <typename T, int L, int MODE> struct Engine {
 #pragma unroll
             for (int z = 0; z < NB; ++z) dft<R>(v + z * R);
             if constexpr (S + 1 < NS) {
+                constexpr int J = L / (P * R);
+                const V* tws = tw + TwLayout<T, L>::offset(S);
 #pragma unroll
                 for (int z = 0; z < NB; ++z) {
                     const int b = tb + TPL * z;
                     const int l = b % P, j1 = b / P;
-                    twiddle<R>(v + z * R, P * j1, tw);
+                    twiddle<R, J>(v + z * R, j1, tws);
 #pragma unroll
                     for (int m = 0; m < R; ++m) sm[sidx(ln, l + P * (m + R * j1))] = v[z * R + m];
                 }

@@ -27,8 +27,11 @@
 #include <vector>
 
 #include "rk_internal.h"
+#include "rk_kernels.cuh"
 
 namespace rk {
+
+constexpr int ilog2_c(int n) { return n <= 1 ? 0 : 1 + ilog2_c(n / 2); }
 
 bool line_info_f32(int L, int mode, int var, LineInfo* out);
 bool line_info_f64(int L, int mode, int var, LineInfo* out);
@@ -52,15 +55,42 @@ bool line_info(int dbl, int L, int mode, int var, LineInfo* out) {
 // ------------------------------------------------------------------------------
 // device tables (FP64 generation)
 // ------------------------------------------------------------------------------
-__global__ void k_gen_tables(float2* twf, double2* twd, float2* hif, float2* lof, double2* hid, double2* lod) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < TWN) {
-        double s, c;
-        // W_TWN^k = exp(-2 pi i k / TWN)
-        sincospi(2.0 * (double)k / (double)TWN, &s, &c);
-        twd[k] = make_double2(c, -s);
-        twf[k] = make_float2((float)c, (float)-s);
+// stage table segment: entries [m - 1][j1] = W_Lp^(j1 m), m in [1, R), j1 < J
+__global__ void k_gen_stage(float2* f, double2* d, int Lp, int R, int J) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (R - 1) * J) return;
+    const int m = e / J + 1, j1 = e % J;
+    const int64_t k = ((int64_t)j1 * m) % Lp;
+    double s, c;
+    sincospi(2.0 * (double)k / (double)Lp, &s, &c);
+    if (d) d[e] = make_double2(c, -s);
+    if (f) f[e] = make_float2((float)c, (float)-s);
+}
+
+struct StageSeg {
+    int64_t off;
+    int Lp, R, J;
+};
+
+template <typename T, int L> static void stage_segs(std::vector<StageSeg>& segs, int64_t base) {
+    using RC = Radix<T, L>;
+    int P = 1;
+    for (int s = 0; s + 1 < RC::NS; ++s) {
+        const int R = RC::R[s];
+        segs.push_back(StageSeg{base + TwLayout<T, L>::offset(s), L / P, R, L / (P * R)});
+        P *= R;
     }
+}
+
+template <typename T, int L, int LMAX> static void stage_layout(std::vector<StageSeg>& segs, int64_t* offs, int64_t& total) {
+    offs[ilog2_c(L)] = total;
+    stage_segs<T, L>(segs, total);
+    total += TwLayout<T, L>::total();
+    if constexpr (L < LMAX) stage_layout<T, 2 * L, LMAX>(segs, offs, total);
+}
+
+__global__ void k_gen_tables(float2* hif, float2* lof, double2* hid, double2* lod) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < TW4_HALF) {
         double s, c;
         sincospi(2.0 * (double)k / (double)(1 << TW4_LOG), &s, &c);
@@ -83,16 +113,29 @@ int device_tables(int device, DeviceTables** out) {
         return RK_OK;
     }
     DeviceTables* t = new DeviceTables();
-    CK(cudaMalloc(&t->tw_f, TWN * sizeof(float2)));
-    CK(cudaMalloc(&t->tw_d, TWN * sizeof(double2)));
+    std::vector<StageSeg> sf, sd;
+    int64_t nf = 0, ndd = 0;
+    stage_layout<float, 1, 16384>(sf, t->off_f, nf);
+    stage_layout<double, 1, 8192>(sd, t->off_d, ndd);
+    CK(cudaMalloc(&t->stw_f, std::max<int64_t>(nf, 1) * sizeof(float2)));
+    CK(cudaMalloc(&t->stw_d, std::max<int64_t>(ndd, 1) * sizeof(double2)));
     CK(cudaMalloc(&t->tw4hi_f, TW4_HALF * sizeof(float2)));
     CK(cudaMalloc(&t->tw4lo_f, TW4_HALF * sizeof(float2)));
     CK(cudaMalloc(&t->tw4hi_d, TW4_HALF * sizeof(double2)));
     CK(cudaMalloc(&t->tw4lo_d, TW4_HALF * sizeof(double2)));
     CK(cudaMalloc(&t->status, sizeof(int32_t)));
     CK(cudaMemset(t->status, 0, sizeof(int32_t)));
-    k_gen_tables<<<TWN / 256, 256>>>((float2*)t->tw_f, (double2*)t->tw_d, (float2*)t->tw4hi_f,
-                                      (float2*)t->tw4lo_f, (double2*)t->tw4hi_d, (double2*)t->tw4lo_d);
+    t->bytes = nf * 8 + ndd * 16 + TW4_HALF * 48;
+    for (const StageSeg& s : sf) {
+        const int n = (s.R - 1) * s.J;
+        k_gen_stage<<<(n + 255) / 256, 256>>>((float2*)t->stw_f + s.off, nullptr, s.Lp, s.R, s.J);
+    }
+    for (const StageSeg& s : sd) {
+        const int n = (s.R - 1) * s.J;
+        k_gen_stage<<<(n + 255) / 256, 256>>>(nullptr, (double2*)t->stw_d + s.off, s.Lp, s.R, s.J);
+    }
+    k_gen_tables<<<TW4_HALF / 256, 256>>>((float2*)t->tw4hi_f, (float2*)t->tw4lo_f, (double2*)t->tw4hi_d,
+                                           (double2*)t->tw4lo_d);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
     g_tabs[device] = t;
@@ -234,6 +277,29 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
     }
 
     const int LM = lane_max(dbl), PM = pos_max(dbl);
+    // the two innermost dims, both transformed powers of two: one clustered pass
+    if (!(d.flags & RK_FLAG_NO_PLANE) && nd >= 2 && axes.size() >= 2 && axes[0] == nd - 1 && axes[1] == nd - 2 &&
+        is_pow2(d.shape[nd - 1]) && is_pow2(d.shape[nd - 2])) {
+        PlaneInfo pi;
+        if (plane_info(dbl, (int)d.shape[nd - 2], (int)d.shape[nd - 1], &pi)) {
+            PassSpec p;
+            p.kind = PK_PLANE;
+            p.L1 = (int)d.shape[nd - 2];
+            p.L2 = (int)d.shape[nd - 1];
+            p.L = p.L2;
+            p.axis = nd - 1;
+            p.axis2 = nd - 2;
+            p.O = prod_range(d.shape, 0, nd - 2);
+            p.ld.buf = cur; p.ld.ax_len = p.L2; p.ld.cA = 0; p.ld.jB = 1;
+            const bool last = axes.size() == 2;
+            const int out = last ? SB_OUT : array_out(true);
+            p.st.buf = out; p.st.ax_len = p.L1; p.st.cA = 0; p.st.jB = 1;
+            p.note = "plane";
+            P.passes.push_back(p);
+            cur = out;
+            axes.erase(axes.begin(), axes.begin() + 2);
+        }
+    }
     for (size_t ai = 0; ai < axes.size(); ++ai) {
         const int ax = axes[ai];
         const int64_t n = d.shape[ax];
@@ -772,7 +838,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         pp.O = ps.O; pp.C = ps.C; pp.I = ps.I;
         pp.nlines = ps.O * ps.C * ps.I;
         build_side(*desc, ps.ld, ps.axis, dbl, true, pp.ld);
-        build_side(*desc, ps.st, ps.axis, dbl, false, pp.st);
+        build_side(*desc, ps.st, ps.kind == PK_PLANE ? ps.axis2 : ps.axis, dbl, false, pp.st);
         if (!r.ld_edge) pp.ld.ptr = bufs[ps.ld.buf];
         if (!r.st_edge) pp.st.ptr = bufs[ps.st.buf];
         if (ps.ld.chirp_axis >= 0) {
@@ -782,39 +848,64 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         }
         if (ps.st.chirp_axis >= 0) pp.st.chirp = blue_tabs[ps.st.chirp_axis].first;
         if (ps.blue_axis >= 0) pp.blue_k = blue_tabs[ps.blue_axis].second;
-        pp.tw = dbl ? tabs->tw_d : tabs->tw_f;
+        {
+            const int lg = ilog2(std::max(ps.L, 1));
+            const int lg2 = ilog2(std::max(ps.kind == PK_PLANE ? ps.L1 : ps.L, 1));
+            if (dbl) {
+                pp.tw = (const double2*)tabs->stw_d + tabs->off_d[lg];
+                pp.tw2 = (const double2*)tabs->stw_d + tabs->off_d[lg2];
+            } else {
+                pp.tw = (const float2*)tabs->stw_f + tabs->off_f[lg];
+                pp.tw2 = (const float2*)tabs->stw_f + tabs->off_f[lg2];
+            }
+        }
         pp.tw4_hi = dbl ? tabs->tw4hi_d : tabs->tw4hi_f;
         pp.tw4_lo = dbl ? tabs->tw4lo_d : tabs->tw4lo_f;
         pp.tw4_N = ps.tw4_N;
         pp.status = tabs->status;
-        LineInfo li;
-        bool ok = line_info(dbl, ps.L, ps.mode, ps.var, &li);
-        if (!ok) {
-            set_error("no kernel instantiation for pass " + ps.note + " L=" + std::to_string(ps.L));
-            return fail(RK_ERR_UNSUPPORTED);
+        r.L1 = ps.L1;
+        r.L2 = ps.L2;
+        r.axis2 = ps.axis2;
+        if (ps.kind == PK_PLANE) {
+            PlaneInfo pi;
+            if (!plane_info(dbl, ps.L1, ps.L2, &pi)) {
+                set_error("no plane kernel instantiation");
+                return fail(RK_ERR_UNSUPPORTED);
+            }
+            r.pi = pi;
+            r.nblocks = ps.O;  // planes
+        } else {
+            LineInfo li;
+            bool ok = line_info(dbl, ps.L, ps.mode, ps.var, &li);
+            if (!ok) {
+                set_error("no kernel instantiation for pass " + ps.note + " L=" + std::to_string(ps.L));
+                return fail(RK_ERR_UNSUPPORTED);
+            }
+            r.nblocks = (pp.nlines + li.nl - 1) / li.nl;
+            r.li = li;
         }
-        r.nblocks = (pp.nlines + li.nl - 1) / li.nl;
-        r.li = li;
         plan->passes.push_back(r);
     }
     if (plan->passes.size() == 1) {
-        // a single pass rewrites only its own lines unless the two edges disagree
-        const Side& a = plan->passes[0].prm.ld;
-        const Side& b = plan->passes[0].prm.st;
-        bool same = a.fmt == b.fmt && a.nd_o == b.nd_o && a.nd_i == b.nd_i && a.ax_stride == b.ax_stride &&
-                    a.ax_shift == b.ax_shift && a.ax_bound == b.ax_bound && a.offset == b.offset;
-        for (int i = 0; same && i < a.nd_o; ++i)
-            same = a.o_stride[i] == b.o_stride[i] && a.o_shift[i] == b.o_shift[i] && a.o_shape[i] == b.o_shape[i] &&
-                   a.o_bound[i] == b.o_bound[i];
-        for (int i = 0; same && i < a.nd_i; ++i)
-            same = a.i_stride[i] == b.i_stride[i] && a.i_shift[i] == b.i_shift[i] && a.i_shape[i] == b.i_shape[i] &&
-                   a.i_bound[i] == b.i_bound[i];
+        // a single pass rewrites only the elements its CTA (or cluster) read, unless the
+        // two edges place the same logical element at different addresses
+        const rk_edge& a = desc->input;
+        const rk_edge& b = desc->output;
+        bool same = a.format == b.format && a.offset == b.offset && a.offset2 == b.offset2;
+        for (int i = 0; same && i < desc->ndim; ++i)
+            same = a.strides[i] == b.strides[i] && a.shift[i] == b.shift[i] && a.shape[i] == b.shape[i] &&
+                   (!fmt_is_pair(a.format) || a.strides2[i] == b.strides2[i]);
         plan->alias_hazard = !same || !plan->passes[0].inplace_safe;
         plan->in_extent_bytes = edge_extent_bytes(desc->input, 0);
         if (fmt_is_pair(desc->input.format)) plan->in2_extent_bytes = edge_extent_bytes(desc->input, 1);
     }
     // set launch attributes now (cudaFuncSetAttribute is not allowed during capture)
-    for (const PassRec& r : plan->passes) CK(r.li.fn(r.prm, 0, nullptr));
+    for (const PassRec& r : plan->passes) {
+        if (r.kind == PK_PLANE)
+            CK(r.pi.fn(r.prm, 0, nullptr));
+        else
+            CK(r.li.fn(r.prm, 0, nullptr));
+    }
     CK(cudaDeviceSynchronize());
     *out = plan;
     return RK_OK;
@@ -973,7 +1064,7 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
         const bool prof = plan->prof_used < plan->prof_max;
         const size_t ev = 2 * ((size_t)plan->prof_used * np + i);
         if (prof) CK(cudaEventRecord(plan->prof_ev[ev], st));
-        cudaError_t e = r.li.fn(p, r.nblocks, st);
+        cudaError_t e = r.kind == PK_PLANE ? r.pi.fn(p, r.nblocks, st) : r.li.fn(p, r.nblocks, st);
         if (e != cudaSuccess) {
             set_error(std::string("kernel launch failed (") + r.note + "): " + cudaGetErrorString(e));
             return RK_ERR_CUDA;

@@ -53,7 +53,8 @@ struct PassParams {
     int64_t O, C, I;      // line decomposition
     int64_t nlines;       // O*C*I
     Side ld, st;
-    const void* tw;       // W_TWN^k, k < TWN (precision of the pass)
+    const void* tw;       // stage twiddle tables of the pass length L (TwLayout)
+    const void* tw2;      // same for the column length of a plane pass
     const void* tw4_hi;   // W_2^24^(4096 k)
     const void* tw4_lo;   // W_2^24^k
     int64_t tw4_N;        // four-step twiddle modulus (power of two <= 2^24)
