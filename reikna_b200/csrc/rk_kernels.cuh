@@ -273,6 +273,69 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
 }
 
 // ------------------------------------------------------------------------------
+// per-thread block load / store: the N elements a thread holds on one line.
+// SF_FAST sides (set by the planner when the side is the pass dtype, the axis
+// index is the position, no padding or cropping along the axis, and only scale /
+// conjugation ops) use one line pointer, 32-bit strided offsets and a power-of-two
+// mask for the index remap; the value ops run once per block with hoisted flags.
+// ------------------------------------------------------------------------------
+template <typename T, int N, class PosF>
+__device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, PosF pos, cplx<T>* v) {
+    using V = cplx<T>;
+    const int32_t f = s.flags;
+    if (f & SF_FAST) {
+        const V* lp = reinterpret_cast<const V*>(s.ptr) + la.base;
+        const int st = (int)s.ax_stride, sh = s.ax_shift, mask = (int)s.ax_len - 1;
+        if (la.ok) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = lp[((pos(i) + sh) & mask) * st];
+        } else {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = cmk<V>(T(0), T(0));
+        }
+        if (f & SF_SCALE) {
+            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
+        }
+        if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = side_load<T>(s, la, pos(i));
+    }
+}
+
+template <typename T, int N, class PosF>
+__device__ __forceinline__ void store_block(const Side& s, const PassParams& p, const LineAddr& la, PosF pos,
+                                            cplx<T>* v) {
+    using V = cplx<T>;
+    const int32_t f = s.flags;
+    if (f & SF_FAST) {
+        if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
+        }
+        if (f & SF_SCALE) {
+            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
+        }
+        if (la.ok) {
+            V* lp = reinterpret_cast<V*>(s.ptr) + la.base;
+            const int st = (int)s.ax_stride, sh = s.ax_shift, mask = (int)s.ax_len - 1;
+#pragma unroll
+            for (int i = 0; i < N; ++i) lp[((pos(i) + sh) & mask) * st] = v[i];
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) side_store<T>(s, p, la, pos(i), v[i]);
+    }
+}
+
+// ------------------------------------------------------------------------------
 // Stockham engine
 // ------------------------------------------------------------------------------
 template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct Engine {
@@ -364,10 +427,7 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassPara
     V v[RT];
     {
         const LineAddr la = line_addr(p.ld, line, p.C, p.I, lok);
-#pragma unroll
-        for (int z = 0; z < RT / R0; ++z)
-#pragma unroll
-            for (int m = 0; m < R0; ++m) v[z * R0 + m] = side_load<T>(p.ld, la, E::in_pos(tb, z, m));
+        load_block<T, RT>(p.ld, la, [&](int i) { return E::in_pos(tb, i / R0, i % R0); }, v);
     }
     E::run(v, sm, ln, tb, tw);
     if constexpr (VAR == 1) {
@@ -408,10 +468,7 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassPara
         }
     } else {
         const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
-#pragma unroll
-        for (int z = 0; z < RT / RL; ++z)
-#pragma unroll
-            for (int m = 0; m < RL; ++m) side_store<T>(p.st, p, la, E::out_pos(tb, z, m), v[z * RL + m]);
+        store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
     }
 }
 

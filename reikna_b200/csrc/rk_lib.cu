@@ -549,6 +549,15 @@ static void build_side(const rk_fft_desc& d, const SideSpec& ss, int ax, int dbl
     }
 }
 
+// Mark a side for the lean block load/store path (load_block / store_block).
+static void mark_fast(Side& s, int dbl, int L) {
+    const int fmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
+    const int32_t bad = SF_CHIRP | SF_TAB | SF_WINDOW | SF_NORM | SF_TW4;
+    if (s.fmt == fmt && s.cA == 0 && s.jB == 1 && s.ax_len == L && s.ax_bound == s.ax_len && is_pow2(L) &&
+        !(s.flags & bad) && s.ax_stride >= 0 && s.ax_stride * (int64_t)L < (int64_t(1) << 31))
+        s.flags |= SF_FAST;
+}
+
 static int validate(const rk_fft_desc* d) {
     if (!d) { set_error("null descriptor"); return RK_ERR_INVALID; }
     if (d->dtype != RK_FMT_C64 && d->dtype != RK_FMT_C128) {
@@ -839,6 +848,8 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         pp.nlines = ps.O * ps.C * ps.I;
         build_side(*desc, ps.ld, ps.axis, dbl, true, pp.ld);
         build_side(*desc, ps.st, ps.kind == PK_PLANE ? ps.axis2 : ps.axis, dbl, false, pp.st);
+        mark_fast(pp.ld, dbl, ps.kind == PK_PLANE ? ps.L2 : ps.L);
+        mark_fast(pp.st, dbl, ps.kind == PK_PLANE ? ps.L1 : ps.L);
         if (!r.ld_edge) pp.ld.ptr = bufs[ps.ld.buf];
         if (!r.st_edge) pp.st.ptr = bufs[ps.st.buf];
         if (ps.ld.chirp_axis >= 0) {

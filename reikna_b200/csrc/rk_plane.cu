@@ -34,7 +34,7 @@ template <typename T, int L1, int L2, int Q> struct PlaneCfg {
 // two resident CTAs per SM (64 registers at 512 threads) so that one cluster's
 // loads overlap another's exchange and stores
 template <typename T, int L1, int L2, int Q>
-__global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, 1024 / PlaneCfg<T, L1, L2, Q>::NT)
+__global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, (sizeof(T) == 4 ? 1024 : 512) / PlaneCfg<T, L1, L2, Q>::NT)
     k_plane(const PassParams p) {
     using V = cplx<T>;
     using C = PlaneCfg<T, L1, L2, Q>;
@@ -56,10 +56,7 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, 1024 / PlaneCfg<T,
         const int ln = tid / ER::TPL, tb = tid % ER::TPL;
         const int64_t line = plane * L1 + (int64_t)q * C::NLR + ln;
         const LineAddr la = line_addr(p.ld, line, 1, 1, pok);
-#pragma unroll
-        for (int z = 0; z < RT / ER::R0; ++z)
-#pragma unroll
-            for (int m = 0; m < ER::R0; ++m) v[z * ER::R0 + m] = side_load<T>(p.ld, la, ER::in_pos(tb, z, m));
+        load_block<T, RT>(p.ld, la, [&](int i) { return ER::in_pos(tb, i / ER::R0, i % ER::R0); }, v);
         ER::run(v, sm, ln, tb, tw);
 #pragma unroll
         for (int z = 0; z < RT / ER::RL; ++z)
@@ -91,10 +88,7 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, 1024 / PlaneCfg<T,
     {
         const int64_t line = plane * L2 + col;
         const LineAddr la = line_addr(p.st, line, 1, L2, pok);
-#pragma unroll
-        for (int z = 0; z < RT / EC::RL; ++z)
-#pragma unroll
-            for (int m = 0; m < EC::RL; ++m) side_store<T>(p.st, p, la, EC::out_pos(tc, z, m), v[z * EC::RL + m]);
+        store_block<T, RT>(p.st, p, la, [&](int i) { return EC::out_pos(tc, i / EC::RL, i % EC::RL); }, v);
     }
 }
 
