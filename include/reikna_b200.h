@@ -70,6 +70,8 @@ extern "C" {
 #define RK_FLAG_NO_PLANE 1   /* never fuse two axes into one clustered pass */
 #define RK_FLAG_NO_BLUE1 2   /* never use the single-pass Bluestein kernel */
 #define RK_FLAG_SPLIT_TC 4   /* tensor-core split-precision radix-16 stages */
+#define RK_FLAG_PLANE_WIDE 8 /* plane pass on twice as many CTAs per cluster (tuning) */
+#define RK_FLAG_NO_TMA 16    /* never use the persistent TMA-fed line passes */
 
 /*
  * One side (input or output) of the FFT as the user sees it after the
@@ -164,6 +166,10 @@ RK_API const char* rk_last_error(void);
 
 /* Library version string. */
 RK_API const char* rk_version(void);
+
+/* Device status word of the current device (nonzero: a kernel gave up a bounded
+ * wait, RK_ERR_DEVICE territory).  Synchronises the device; clear = 1 resets it. */
+RK_API int rk_device_status(int32_t* status, int32_t clear);
 
 /* sizeof(rk_edge) and sizeof(rk_fft_desc) as compiled, for binding checks. */
 RK_API int rk_abi_sizes(int64_t* edge_bytes, int64_t* desc_bytes);

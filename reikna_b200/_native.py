@@ -38,6 +38,8 @@ WIN_HANN = 1
 FLAG_NO_PLANE = 1
 FLAG_NO_BLUE1 = 2
 FLAG_SPLIT_TC = 4
+FLAG_PLANE_WIDE = 8
+FLAG_NO_TMA = 16
 
 EXPORTED = (
     "rk_edge_init",
@@ -53,6 +55,7 @@ EXPORTED = (
     "rk_abi_sizes",
     "rk_fft_profile",
     "rk_fft_profile_read",
+    "rk_device_status",
 )
 
 I64A = ctypes.c_int64 * MAXD
@@ -166,6 +169,7 @@ def lib() -> ctypes.CDLL:
         ]
         L.rk_abi_sizes.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
         L.rk_fft_profile.argtypes = [vp, ctypes.c_int32]
+        L.rk_device_status.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
         L.rk_fft_profile_read.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
         L.rk_last_error.restype = ctypes.c_char_p
         L.rk_version.restype = ctypes.c_char_p

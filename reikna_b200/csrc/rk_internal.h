@@ -22,6 +22,17 @@ struct LineInfo {
     size_t smem;   // dynamic shared memory bytes
 };
 
+struct TmaInfo {
+    LineLaunch fn;
+    int (*per_sm)();   // resident CTAs per SM
+    int nt;
+    int nl;
+    size_t smem;
+};
+bool tma_info(int dbl, int L, int mode, TmaInfo* out);
+bool encode_lane_map(void* base, int dbl, int64_t I, int64_t L, int64_t O, int64_t sj, int64_t so, int nl, int rows,
+                     TensorMapBytes* out);
+
 struct PlaneInfo {
     PlaneLaunch fn;
     int q;         // cluster size
@@ -31,7 +42,7 @@ struct PlaneInfo {
 
 // lookup; returns false if the combination is not compiled
 bool line_info(int dbl, int L, int mode, int var, LineInfo* out);
-bool plane_info(int dbl, int L1, int L2, PlaneInfo* out);
+bool plane_info(int dbl, int L1, int L2, int wide, PlaneInfo* out);
 
 struct PassRec {
     int kind = PK_LINE;
@@ -48,6 +59,11 @@ struct PassRec {
     int64_t nblocks = 0;
     LineInfo li{};
     PlaneInfo pi{};
+    TmaInfo ti{};
+    bool use_tma = false;
+    bool tma_reencode = false;     // tensor map over the user's input: re-encode per call
+    const void* tma_ptr = nullptr; // pointer the current map was encoded for
+    int tma_rows = 0;
     std::string note;
 };
 

@@ -281,7 +281,7 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
     if (!(d.flags & RK_FLAG_NO_PLANE) && nd >= 2 && axes.size() >= 2 && axes[0] == nd - 1 && axes[1] == nd - 2 &&
         is_pow2(d.shape[nd - 1]) && is_pow2(d.shape[nd - 2])) {
         PlaneInfo pi;
-        if (plane_info(dbl, (int)d.shape[nd - 2], (int)d.shape[nd - 1], &pi)) {
+        if (plane_info(dbl, (int)d.shape[nd - 2], (int)d.shape[nd - 1], (d.flags & RK_FLAG_PLANE_WIDE) ? 1 : 0, &pi)) {
             PassSpec p;
             p.kind = PK_PLANE;
             p.L1 = (int)d.shape[nd - 2];
@@ -558,6 +558,54 @@ static void mark_fast(Side& s, int dbl, int L) {
         s.flags |= SF_FAST;
 }
 
+// Switch a plain line pass to the persistent TMA-fed kernel when its load side is a
+// whole-tile, 16-byte aligned layout (see rk_tma.cu).  Tensor maps over plan
+// temporaries are encoded here; over the user's input they are encoded per call.
+static void setup_tma(PassRec& r, int dbl, int nsm) {
+    PassParams& p = r.prm;
+    const Side& ld = p.ld;
+    const Side& st = p.st;
+    const int esz = dbl ? 16 : 8;
+    if (!(ld.flags & SF_FAST) || !(st.flags & SF_FAST) || ld.ax_shift != 0 || p.C != 1) return;
+    TmaInfo ti;
+    if (!tma_info(dbl, r.L, r.mode, &ti)) return;
+    const int64_t L = r.L, NL = ti.nl;
+    for (int i = 0; i < ld.nd_o; ++i)
+        if (ld.o_shift[i] != 0 || ld.o_bound[i] != ld.o_shape[i]) return;
+    if (r.mode == MODE_POS) {
+        if (p.I != 1 || ld.nd_i != 0 || ld.ax_stride != 1 || ld.nd_o > 1) return;
+        if (ld.nd_o == 1 && ld.o_stride[0] != L) return;
+        if ((ld.offset * esz) % 16 != 0 || (L * esz) % 16 != 0) return;
+        p.tma_mode = TMA_BULK;
+        p.tile_stride = NL * L;
+    } else {
+        if (p.I % NL != 0 || ld.nd_i != 1 || ld.i_stride[0] != 1 || ld.i_shape[0] != p.I || ld.i_shift[0] != 0 ||
+            ld.i_bound[0] != p.I || ld.nd_o > 1)
+            return;
+        if ((ld.ax_stride * esz) % 16 != 0) return;
+        if (ld.nd_o == 1 && (ld.o_stride[0] * esz) % 16 != 0) return;
+        if (ld.offset != 0) return;
+        p.tma_mode = TMA_TENSOR;
+        p.tma_boxes = (int)std::max<int64_t>(1, L / 256);
+        r.tma_rows = (int)(L / p.tma_boxes);
+        if (ld.ptr) {
+            const int64_t so = ld.nd_o == 1 ? ld.o_stride[0] : L * p.I;
+            if (!encode_lane_map(ld.ptr, dbl, p.I, L, p.O, ld.ax_stride, so, (int)NL, r.tma_rows, &p.tmap)) {
+                p.tma_mode = TMA_NONE;
+                return;
+            }
+            r.tma_ptr = ld.ptr;
+        } else {
+            r.tma_reencode = true;
+        }
+    }
+    p.ntiles = (p.nlines + NL - 1) / NL;
+    const int per = std::max(1, ti.per_sm());
+    r.nblocks = std::min<int64_t>(p.ntiles, (int64_t)nsm * per);
+    r.ti = ti;
+    r.use_tma = true;
+}
+
 static int validate(const rk_fft_desc* d) {
     if (!d) { set_error("null descriptor"); return RK_ERR_INVALID; }
     if (d->dtype != RK_FMT_C64 && d->dtype != RK_FMT_C128) {
@@ -665,6 +713,22 @@ extern "C" {
 const char* rk_last_error(void) { return g_err.c_str(); }
 const char* rk_version(void) { return "reikna_b200 0.1.0 (sm_100a)"; }
 
+int rk_device_status(int32_t* status, int32_t clear) {
+    if (!status) {
+        set_error("null argument");
+        return RK_ERR_INVALID;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    DeviceTables* t = nullptr;
+    int rc = device_tables(dev, &t);
+    if (rc) return rc;
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(status, t->status, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (clear) CK(cudaMemset(t->status, 0, sizeof(int32_t)));
+    return RK_OK;
+}
+
 int rk_abi_sizes(int64_t* edge_bytes, int64_t* desc_bytes) {
     if (!edge_bytes || !desc_bytes) {
         set_error("null argument");
@@ -735,6 +799,8 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
 
     int dev = 0;
     CK(cudaGetDevice(&dev));
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     DeviceTables* tabs = nullptr;
     rc = device_tables(dev, &tabs);
     if (rc) return rc;
@@ -879,7 +945,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         r.axis2 = ps.axis2;
         if (ps.kind == PK_PLANE) {
             PlaneInfo pi;
-            if (!plane_info(dbl, ps.L1, ps.L2, &pi)) {
+            if (!plane_info(dbl, ps.L1, ps.L2, (desc->flags & RK_FLAG_PLANE_WIDE) ? 1 : 0, &pi)) {
                 set_error("no plane kernel instantiation");
                 return fail(RK_ERR_UNSUPPORTED);
             }
@@ -894,6 +960,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             }
             r.nblocks = (pp.nlines + li.nl - 1) / li.nl;
             r.li = li;
+            if (!(desc->flags & RK_FLAG_NO_TMA) && ps.var == 0) setup_tma(r, dbl, nsm);
         }
         plan->passes.push_back(r);
     }
@@ -916,6 +983,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             CK(r.pi.fn(r.prm, 0, nullptr));
         else
             CK(r.li.fn(r.prm, 0, nullptr));
+        if (r.use_tma) CK(r.ti.fn(r.prm, 0, nullptr));
     }
     CK(cudaDeviceSynchronize());
     *out = plan;
@@ -1045,7 +1113,23 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
     }
     const size_t np = plan->passes.size();
     for (size_t i = 0; i < np; ++i) {
-        const PassRec& r = plan->passes[i];
+        PassRec& r = plan->passes[i];
+        bool tma = r.use_tma;
+        if (tma && r.ld_edge) {
+            // a view of the user's array may start off the 16-byte grid the bulk
+            // copies need: such calls take the plain kernel
+            const int esz = r.dbl ? 16 : 8;
+            if ((((uintptr_t)in0) + (uintptr_t)(r.prm.ld.offset * esz)) % 16 != 0) tma = false;
+        }
+        if (tma && r.tma_reencode && r.tma_ptr != in0) {
+            const Side& ld = r.prm.ld;
+            const int64_t so = ld.nd_o == 1 ? ld.o_stride[0] : (int64_t)r.L * r.prm.I;
+            if (encode_lane_map(const_cast<void*>(in0), r.dbl, r.prm.I, r.L, r.prm.O, ld.ax_stride, so, r.ti.nl,
+                                r.tma_rows, &r.prm.tmap))
+                r.tma_ptr = in0;
+            else
+                tma = false;
+        }
         PassParams p = r.prm;
         if (r.ld_edge) {
             p.ld.ptr = const_cast<void*>(in0);
@@ -1075,7 +1159,9 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
         const bool prof = plan->prof_used < plan->prof_max;
         const size_t ev = 2 * ((size_t)plan->prof_used * np + i);
         if (prof) CK(cudaEventRecord(plan->prof_ev[ev], st));
-        cudaError_t e = r.kind == PK_PLANE ? r.pi.fn(p, r.nblocks, st) : r.li.fn(p, r.nblocks, st);
+        cudaError_t e = tma                  ? r.ti.fn(p, r.nblocks, st)
+                        : r.kind == PK_PLANE ? r.pi.fn(p, r.nblocks, st)
+                                             : r.li.fn(p, (p.nlines + r.li.nl - 1) / r.li.nl, st);
         if (e != cudaSuccess) {
             set_error(std::string("kernel launch failed (") + r.note + "): " + cudaGetErrorString(e));
             return RK_ERR_CUDA;

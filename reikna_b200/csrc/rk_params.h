@@ -50,7 +50,19 @@ struct Side {
     const void* tab;
 };
 
+// opaque 128-byte CUtensorMap (encoded on the host with cuTensorMapEncodeTiled)
+struct alignas(64) TensorMapBytes {
+    uint64_t w[16];
+};
+
+enum TmaMode : int32_t { TMA_NONE = 0, TMA_BULK = 1, TMA_TENSOR = 2 };
+
 struct PassParams {
+    TensorMapBytes tmap;  // load-side tensor map (TMA_TENSOR)
+    int32_t tma_mode;     // TmaMode of the persistent pipelined kernel
+    int32_t tma_boxes;    // tensor copies per tile (L split in boxes of <= 256 rows)
+    int64_t ntiles;       // tiles of NL lines
+    int64_t tile_stride;  // TMA_BULK: elements between consecutive tiles' first lines
     int64_t O, C, I;      // line decomposition
     int64_t nlines;       // O*C*I
     Side ld, st;

@@ -2,13 +2,15 @@
 // round trip, using a thread-block cluster and distributed shared memory.
 //
 // A cluster of Q CTAs owns one L1 x L2 plane.  CTA q loads rows [q L1/Q, (q+1) L1/Q)
-// (contiguous, coalesced), transforms them along the last axis and leaves the row
-// spectra in its shared memory.  After a cluster barrier every CTA gathers its
-// L2/Q columns from all Q CTAs' shared memory (ld.shared::cluster through
-// map_shared_rank), transforms them along the row axis and stores them (adjacent
-// columns are adjacent in memory, so the stores coalesce).  A 256^3 complex64
-// transform is then two HBM passes (this one plus one strided pass) instead of
-// reikna's five kernels (reikna/fft/fft.py:532-584 for the chain it builds).
+// (contiguous, coalesced) and transforms them along the last axis.  After a
+// cluster barrier (every CTA is done with its own shared memory) each thread pushes
+// its row spectra straight into the shared memory of the CTA that owns those
+// columns (st.shared::cluster through map_shared_rank, laid out for the column
+// phase), so no thread waits on a remote read.  After a second barrier every CTA
+// transforms its L2/Q columns along the row axis and stores them (adjacent columns
+// are adjacent in memory, so the stores coalesce).  A 256^3 complex64 transform is
+// then two HBM passes (this one plus one strided pass) instead of reikna's five
+// kernels (reikna/fft/fft.py:532-584 for the chain it builds).
 #include <cooperative_groups.h>
 
 #include "rk_internal.h"
@@ -29,12 +31,12 @@ template <typename T, int L1, int L2, int Q> struct PlaneCfg {
     static constexpr int LS2 = L2 + L2 / 16;
     static constexpr int A = NLR * LS2, B = NLC * L1;
     static constexpr size_t SMEM = (size_t)(A > B ? A : B) * ESZ;
+    // resident CTAs per SM the register budget is sized for
+    static constexpr int MINB = (sizeof(T) == 4 ? 1024 : 512) / NT > 0 ? (sizeof(T) == 4 ? 1024 : 512) / NT : 1;
 };
 
-// two resident CTAs per SM (64 registers at 512 threads) so that one cluster's
-// loads overlap another's exchange and stores
 template <typename T, int L1, int L2, int Q>
-__global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, (sizeof(T) == 4 ? 1024 : 512) / PlaneCfg<T, L1, L2, Q>::NT)
+__global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, PlaneCfg<T, L1, L2, Q>::MINB)
     k_plane(const PassParams p) {
     using V = cplx<T>;
     using C = PlaneCfg<T, L1, L2, Q>;
@@ -52,38 +54,42 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, (sizeof(T) == 4 ? 
 
     V v[RT];
     // ---- rows: transform along the last axis
+    const int ln = tid / ER::TPL, tb = tid % ER::TPL;
     {
-        const int ln = tid / ER::TPL, tb = tid % ER::TPL;
         const int64_t line = plane * L1 + (int64_t)q * C::NLR + ln;
         const LineAddr la = line_addr(p.ld, line, 1, 1, pok);
         load_block<T, RT>(p.ld, la, [&](int i) { return ER::in_pos(tb, i / ER::R0, i % ER::R0); }, v);
         ER::run(v, sm, ln, tb, tw);
-#pragma unroll
-        for (int z = 0; z < RT / ER::RL; ++z)
-#pragma unroll
-            for (int m = 0; m < ER::RL; ++m) sm[ER::sidx(ln, ER::out_pos(tb, z, m))] = v[z * ER::RL + m];
     }
     if constexpr (Q > 1)
         cg::this_cluster().sync();
     else
         __syncthreads();
-    // ---- columns: gather from every CTA of the cluster, transform along the row axis
+    // ---- push row spectra into the owners of their columns (column-phase layout)
+    {
+        const int row = q * C::NLR + ln;
+#pragma unroll
+        for (int z = 0; z < RT / ER::RL; ++z)
+#pragma unroll
+            for (int m = 0; m < ER::RL; ++m) {
+                const int col = ER::out_pos(tb, z, m);
+                V* dst = sm;
+                if constexpr (Q > 1) dst = cg::this_cluster().map_shared_rank(sm, col / C::NLC);
+                dst[EC::sidx(col % C::NLC, row)] = v[z * ER::RL + m];
+            }
+    }
+    if constexpr (Q > 1)
+        cg::this_cluster().sync();
+    else
+        __syncthreads();
+    // ---- columns: transform along the row axis
     const int lc = tid % C::NLC, tc = tid / C::NLC;
     const int col = q * C::NLC + lc;
 #pragma unroll
     for (int z = 0; z < RT / EC::R0; ++z)
 #pragma unroll
-        for (int m = 0; m < EC::R0; ++m) {
-            const int r = EC::in_pos(tc, z, m);
-            const int owner = r / C::NLR, lr = r % C::NLR;
-            const V* src = sm;
-            if constexpr (Q > 1) src = cg::this_cluster().map_shared_rank(sm, owner);
-            v[z * EC::R0 + m] = src[ER::sidx(lr, col)];
-        }
-    if constexpr (Q > 1)
-        cg::this_cluster().sync();
-    else
-        __syncthreads();
+        for (int m = 0; m < EC::R0; ++m) v[z * EC::R0 + m] = sm[EC::sidx(lc, EC::in_pos(tc, z, m))];
+    __syncthreads();
     EC::run(v, sm, lc, tc, reinterpret_cast<const V*>(p.tw2));
     {
         const int64_t line = plane * L2 + col;
@@ -125,13 +131,23 @@ template <typename T, int L1, int L2, int Q> struct PlaneLauncher {
     static PlaneInfo info() { return PlaneInfo{&launch, Q, C::NT, C::SMEM}; }
 };
 
-bool plane_info(int dbl, int L1, int L2, PlaneInfo* out) {
+// wide = 1 selects the 16-CTA cluster variant where one exists
+bool plane_info(int dbl, int L1, int L2, int wide, PlaneInfo* out) {
     if (!dbl) {
-        if (L1 == 256 && L2 == 256) { *out = PlaneLauncher<float, 256, 256, 8>::info(); return true; }
-        if (L1 == 128 && L2 == 128) { *out = PlaneLauncher<float, 128, 128, 2>::info(); return true; }
+        if (L1 == 256 && L2 == 256) {
+            *out = wide ? PlaneLauncher<float, 256, 256, 16>::info() : PlaneLauncher<float, 256, 256, 8>::info();
+            return true;
+        }
+        if (L1 == 128 && L2 == 128) {
+            *out = wide ? PlaneLauncher<float, 128, 128, 4>::info() : PlaneLauncher<float, 128, 128, 2>::info();
+            return true;
+        }
         if (L1 == 64 && L2 == 64) { *out = PlaneLauncher<float, 64, 64, 1>::info(); return true; }
     } else {
-        if (L1 == 128 && L2 == 128) { *out = PlaneLauncher<double, 128, 128, 4>::info(); return true; }
+        if (L1 == 128 && L2 == 128) {
+            *out = wide ? PlaneLauncher<double, 128, 128, 8>::info() : PlaneLauncher<double, 128, 128, 4>::info();
+            return true;
+        }
         if (L1 == 64 && L2 == 64) { *out = PlaneLauncher<double, 64, 64, 1>::info(); return true; }
     }
     return false;

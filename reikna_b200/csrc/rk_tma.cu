@@ -1,0 +1,225 @@
+// Persistent line passes fed by the Tensor Memory Accelerator.
+//
+// Each CTA loops over tiles of NL lines.  Two shared-memory buffers alternate: while
+// the CTA transforms tile k out of one buffer, the bulk-copy engine is already
+// writing tile k+1 into the other (completion tracked by an mbarrier per buffer), so
+// HBM latency overlaps the butterflies instead of stalling the warps that issued the
+// loads.  The buffer of the current tile doubles as the Stockham exchange buffer
+// once its stage-0 inputs are in registers.  Results are stored straight from
+// registers (coalesced 128-byte rows), then the freed buffer receives tile k+2.
+//
+//  * position mode: a tile is NL contiguous lines -> one 1-D cp.async.bulk;
+//  * lane mode: a tile is L rows of NL adjacent lines (128 bytes) at the axis
+//    stride -> a 3-D tiled tensor copy whose box lands in shared memory exactly in
+//    the lane-mode layout [position][lane].
+#include <cuda.h>
+
+#include <mutex>
+
+#include "rk_async.cuh"
+#include "rk_internal.h"
+#include "rk_kernels.cuh"
+
+namespace rk {
+
+template <typename T, int L, int MODE> struct TmaCfg {
+    using Cfg = LineCfg<T, L, MODE>;
+    static constexpr int NL = Cfg::NL, NT = Cfg::NT, ESZ = Cfg::ESZ;
+    static constexpr int TILE = NL * L;                                           // elements copied
+    static constexpr int BUF = MODE == MODE_POS ? NL * Cfg::LS : NL * L;          // elements per buffer
+    static constexpr size_t SMEM = 2 * (size_t)BUF * ESZ + 64;                     // + 2 mbarriers
+};
+
+template <typename T, int L, int MODE>
+__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line_tma(const __grid_constant__ PassParams p) {
+    using V = cplx<T>;
+    using E = Engine<T, L, MODE>;
+    using C = TmaCfg<T, L, MODE>;
+    constexpr int RT = E::RT, TPL = E::TPL, NL = E::NL, R0 = E::R0, RL = E::RL;
+    extern __shared__ __align__(128) unsigned char rk_smem[];
+    V* buf0 = reinterpret_cast<V*>(rk_smem);
+    V* buf1 = buf0 + C::BUF;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(buf1 + C::BUF);
+    const V* tw = reinterpret_cast<const V*>(p.tw);
+    const int tid = threadIdx.x;
+    const int ln = MODE == MODE_POS ? tid / TPL : tid % NL;
+    const int tb = MODE == MODE_POS ? tid % TPL : tid / NL;
+
+    auto issue = [&](int64_t t, int b) {
+        V* dst = b ? buf1 : buf0;
+        uint64_t* bar = bars + b;
+        if (p.tma_mode == TMA_BULK) {
+            const int64_t first = t * NL;
+            const int64_t nl = (p.nlines - first) < NL ? (p.nlines - first) : NL;
+            const uint32_t bytes = (uint32_t)(nl * L * C::ESZ);
+            mbar_arrive_expect_tx(bar, bytes);
+            const V* src = reinterpret_cast<const V*>(p.ld.ptr) + p.ld.offset + t * p.tile_stride;
+            bulk_g2s(dst, src, bytes, bar);
+        } else {
+            const int64_t first = t * NL;
+            const int64_t o = first / p.I, i = first % p.I;
+            const int rows = L / p.tma_boxes;
+            mbar_arrive_expect_tx(bar, (uint32_t)(C::TILE * C::ESZ));
+            const int xs = sizeof(T) == 8 ? 2 : 1;  // complex128 maps as pairs of doubles
+            for (int k = 0; k < p.tma_boxes; ++k)
+                tma_g2s_3d(dst + (size_t)k * rows * NL, &p.tmap, (int)i * xs, k * rows, (int)o, bar);
+        }
+    };
+
+    if (tid == 0) {
+        mbar_init(bars + 0, 1);
+        mbar_init(bars + 1, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const int64_t stride = gridDim.x;
+    int64_t t = blockIdx.x;
+    if (tid == 0) {
+        if (t < p.ntiles) issue(t, 0);
+        if (t + stride < p.ntiles) issue(t + stride, 1);
+    }
+    uint32_t phase0 = 0, phase1 = 0;
+    for (int k = 0; t < p.ntiles; t += stride, ++k) {
+        const int b = k & 1;
+        V* buf = b ? buf1 : buf0;
+        const bool ok = mbar_wait(bars + b, b ? phase1 : phase0, p.status);
+        if (b) phase1 ^= 1; else phase0 ^= 1;
+        if (!ok) {
+            // the status word records the timeout; before leaving, give the copy into
+            // the other buffer (if one was issued) a bounded chance to land
+            if (t + stride < p.ntiles) mbar_wait(bars + (b ^ 1), b ? phase0 : phase1, nullptr);
+            break;
+        }
+        V v[RT];
+#pragma unroll
+        for (int z = 0; z < RT / R0; ++z)
+#pragma unroll
+            for (int m = 0; m < R0; ++m) {
+                const int pos = E::in_pos(tb, z, m);
+                v[z * R0 + m] = MODE == MODE_POS ? buf[ln * L + pos] : buf[pos * NL + ln];
+            }
+        if (p.ld.flags & SF_SCALE) {
+            const V c = cmk<V>((T)p.ld.scale_re, (T)p.ld.scale_im);
+#pragma unroll
+            for (int i = 0; i < RT; ++i) v[i] = cmul(v[i], c);
+        }
+        if (((p.ld.flags & SF_PRE_CONJ) != 0) != ((p.ld.flags & SF_POST_CONJ) != 0)) {
+#pragma unroll
+            for (int i = 0; i < RT; ++i) v[i].y = -v[i].y;
+        }
+        __syncthreads();  // the tile is in registers: the buffer becomes the exchange area
+        E::run(v, buf, ln, tb, tw);
+        if constexpr (E::NS == 1) __syncthreads();
+        if (tid == 0 && t + 2 * stride < p.ntiles) {
+            fence_proxy_async_smem();
+            issue(t + 2 * stride, b);
+        }
+        const int64_t line = t * NL + ln;
+        const LineAddr la = line_addr(p.st, line, p.C, p.I, line < p.nlines);
+        store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
+    }
+}
+
+template <typename T, int L, int MODE> struct TmaLauncher {
+    using C = TmaCfg<T, L, MODE>;
+    static cudaError_t launch(const PassParams& p, int64_t nblocks, cudaStream_t st) {
+        static bool attr_done = false;
+        if (!attr_done) {
+            cudaError_t e =
+                cudaFuncSetAttribute(k_line_tma<T, L, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+            if (e != cudaSuccess) return e;
+            attr_done = true;
+        }
+        if (nblocks <= 0) return cudaSuccess;
+        k_line_tma<T, L, MODE><<<(unsigned)nblocks, C::NT, C::SMEM, st>>>(p);
+        return cudaGetLastError();
+    }
+    static int per_sm() {
+        int n = 0;
+        cudaFuncSetAttribute(k_line_tma<T, L, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_line_tma<T, L, MODE>, C::NT, C::SMEM);
+        return n;
+    }
+    static TmaInfo info() { return TmaInfo{&launch, &per_sm, C::NT, C::NL, C::SMEM}; }
+};
+
+#define RK_TI(TY, LL, MODE) \
+    if (L == LL && mode == MODE) { *out = TmaLauncher<TY, LL, MODE>::info(); return true; }
+
+bool tma_info(int dbl, int L, int mode, TmaInfo* out) {
+    if (!dbl) {
+        RK_TI(float, 64, MODE_POS)
+        RK_TI(float, 128, MODE_POS)
+        RK_TI(float, 256, MODE_POS)
+        RK_TI(float, 512, MODE_POS)
+        RK_TI(float, 1024, MODE_POS)
+        RK_TI(float, 2048, MODE_POS)
+        RK_TI(float, 4096, MODE_POS)
+        RK_TI(float, 8192, MODE_POS)
+        RK_TI(float, 16, MODE_LANE)
+        RK_TI(float, 32, MODE_LANE)
+        RK_TI(float, 64, MODE_LANE)
+        RK_TI(float, 128, MODE_LANE)
+        RK_TI(float, 256, MODE_LANE)
+        RK_TI(float, 512, MODE_LANE)
+        RK_TI(float, 1024, MODE_LANE)
+    } else {
+        RK_TI(double, 64, MODE_POS)
+        RK_TI(double, 128, MODE_POS)
+        RK_TI(double, 256, MODE_POS)
+        RK_TI(double, 512, MODE_POS)
+        RK_TI(double, 1024, MODE_POS)
+        RK_TI(double, 2048, MODE_POS)
+        RK_TI(double, 4096, MODE_POS)
+        RK_TI(double, 16, MODE_LANE)
+        RK_TI(double, 32, MODE_LANE)
+        RK_TI(double, 64, MODE_LANE)
+        RK_TI(double, 128, MODE_LANE)
+        RK_TI(double, 256, MODE_LANE)
+        RK_TI(double, 512, MODE_LANE)
+    }
+    return false;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// 3-D map over (line-in-plane i, position, plane o) of a lane-mode load side:
+// element (o, i, j) at base + (o * so + i + j * sj) elements.  Box {NL, rows, 1}.
+bool encode_lane_map(void* base, int dbl, int64_t I, int64_t L, int64_t O, int64_t sj, int64_t so, int nl, int rows,
+                     TensorMapBytes* out) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const int xs = dbl ? 2 : 1;  // complex128 as two doubles, complex64 as one 64-bit word
+    const int64_t esz = dbl ? 8 : 8;
+    cuuint64_t dims[3] = {(cuuint64_t)(I * xs), (cuuint64_t)L, (cuuint64_t)O};
+    cuuint64_t strides[2] = {(cuuint64_t)(sj * xs * esz), (cuuint64_t)(so * xs * esz)};
+    cuuint32_t box[3] = {(cuuint32_t)(nl * xs), (cuuint32_t)rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    if (strides[0] % 16 || strides[1] % 16 || ((uintptr_t)base) % 16) return false;
+    CUtensorMap m;
+    CUresult r = fn(&m, dbl ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, base, dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    static_assert(sizeof(CUtensorMap) == sizeof(TensorMapBytes), "tensor map size");
+    memcpy(out, &m, sizeof(m));
+    return true;
+}
+
+}  // namespace rk

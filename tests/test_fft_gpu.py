@@ -151,6 +151,33 @@ def test_trivial(rng):
     assert diff_is_negligible(res.cpu().numpy(), x * 4, 1e-8, 1e-5)
 
 
+@pytest.mark.parametrize("shape,axes", [((65, 1024), (1,)), ((3, 257, 256, 16), (2,)), ((9, 64, 64), (1, 2))])
+def test_misaligned_views(rng, shape, axes):
+    # views starting 8 bytes into an allocation take the non-TMA path
+    from reikna_b200.fft import FFT
+
+    torch = _torch()
+    x = uniform_array(rng, shape, numpy.complex64)
+    base = to_dev(x)
+    t = base[1:]
+    out = torch.empty_like(t)
+    c = FFT(t, axes=axes).compile()
+    c(None, out, t)
+    torch.cuda.synchronize()
+    ref = numpy.fft.fftn(x[1:].astype(numpy.complex128), axes=axes)
+    assert rel_l2(out.cpu().numpy(), ref) < fft_bound(numpy.complex64, math.prod(shape[a] for a in axes))
+
+
+def test_device_status_clear():
+    import ctypes
+
+    from reikna_b200 import _native as N
+
+    s = ctypes.c_int32(-1)
+    N.check(N.lib().rk_device_status(ctypes.byref(s), 1))
+    assert s.value == 0
+
+
 def test_strided_input_view(rng):
     from reikna_b200.fft import FFT
 
