@@ -49,12 +49,72 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
+// about one second of SM clock: no legitimate wait in these kernels comes near it
+constexpr long long RK_WAIT_CYCLES = 2000000000LL;
+
 // bounded wait on phase `parity`; false (and the status bit set) on timeout
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* status) {
-    for (uint32_t i = 0; i < RK_WAIT_LIMIT; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    for (uint32_t i = 0; i < RK_WAIT_LIMIT; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (clock64() - t0 > RK_WAIT_CYCLES) break;
+    }
     if (status) atomicOr(status, RK_STATUS_TIMEOUT);
     return false;
+}
+
+// same, acquiring at cluster scope (data and arrivals from other CTAs of the cluster)
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, int32_t* status) {
+    if (mbar_try_wait_cluster(bar, parity)) return true;
+    const long long t0 = clock64();
+    for (uint32_t i = 0; i < RK_WAIT_LIMIT; ++i) {
+        if (mbar_try_wait_cluster(bar, parity)) return true;
+        if (clock64() - t0 > RK_WAIT_CYCLES) break;
+    }
+    if (status) atomicOr(status, RK_STATUS_TIMEOUT);
+    return false;
+}
+
+// shared::cluster address of the same shared variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t mapa(uint32_t local_addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local_addr), "r"(rank));
+    return r;
+}
+
+// arrive on an mbarrier of another CTA of the cluster (release at cluster scope)
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+// asynchronous store into another CTA's shared memory whose bytes complete the
+// transaction count of that CTA's mbarrier
+__device__ __forceinline__ void st_async(uint32_t cluster_addr, float2 v, uint32_t cluster_bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(
+                     cluster_addr),
+                 "f"(v.x), "f"(v.y), "r"(cluster_bar)
+                 : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t cluster_addr, double2 v, uint32_t cluster_bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(
+                     cluster_addr),
+                 "d"(v.x), "d"(v.y), "r"(cluster_bar)
+                 : "memory");
 }
 
 // 1-D bulk copy global -> shared, completion counted on `bar` (bytes % 16 == 0,

@@ -33,6 +33,15 @@ bool tma_info(int dbl, int L, int mode, TmaInfo* out);
 bool encode_lane_map(void* base, int dbl, int64_t I, int64_t L, int64_t O, int64_t sj, int64_t so, int nl, int rows,
                      TensorMapBytes* out);
 
+struct PlaneTmaInfo {
+    LineLaunch fn;        // nblocks = CTAs of the persistent grid
+    int (*clusters)();    // clusters resident at once
+    int q;
+    int nt;
+    size_t smem;
+};
+bool plane_tma_info(int dbl, int L1, int L2, PlaneTmaInfo* out);
+
 struct PlaneInfo {
     PlaneLaunch fn;
     int q;         // cluster size
@@ -60,6 +69,9 @@ struct PassRec {
     LineInfo li{};
     PlaneInfo pi{};
     TmaInfo ti{};
+    PlaneTmaInfo pti{};
+    bool use_plane_tma = false;
+    int64_t plane_tma_blocks = 0;
     bool use_tma = false;
     bool tma_reencode = false;     // tensor map over the user's input: re-encode per call
     const void* tma_ptr = nullptr; // pointer the current map was encoded for

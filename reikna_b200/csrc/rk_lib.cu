@@ -951,6 +951,22 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             }
             r.pi = pi;
             r.nblocks = ps.O;  // planes
+            PlaneTmaInfo pti;
+            const Side& ld = pp.ld;
+            const int esz = dbl ? 16 : 8;
+            bool ok_tma = !(desc->flags & (RK_FLAG_NO_TMA | RK_FLAG_PLANE_WIDE)) &&
+                          plane_tma_info(dbl, ps.L1, ps.L2, &pti) && (ld.flags & SF_FAST) && ld.ax_shift == 0 &&
+                          ld.ax_stride == 1 && ld.nd_i == 0 && ld.nd_o == 1 && ld.o_stride[0] == ps.L2 &&
+                          ld.o_shift[0] == 0 && ld.o_bound[0] == ld.o_shape[0] && (ld.offset * esz) % 16 == 0;
+            if (ok_tma) {
+                const int ncl = pti.clusters();
+                if (ncl > 0) {
+                    pp.tile_stride = (int64_t)ps.L1 * ps.L2;
+                    r.pti = pti;
+                    r.use_plane_tma = true;
+                    r.plane_tma_blocks = std::min<int64_t>(ps.O, ncl) * pti.q;
+                }
+            }
         } else {
             LineInfo li;
             bool ok = line_info(dbl, ps.L, ps.mode, ps.var, &li);
@@ -984,6 +1000,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         else
             CK(r.li.fn(r.prm, 0, nullptr));
         if (r.use_tma) CK(r.ti.fn(r.prm, 0, nullptr));
+        if (r.use_plane_tma) CK(r.pti.fn(r.prm, 0, nullptr));
     }
     CK(cudaDeviceSynchronize());
     *out = plan;
@@ -1114,7 +1131,7 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
     const size_t np = plan->passes.size();
     for (size_t i = 0; i < np; ++i) {
         PassRec& r = plan->passes[i];
-        bool tma = r.use_tma;
+        bool tma = r.use_tma || r.use_plane_tma;
         if (tma && r.ld_edge) {
             // a view of the user's array may start off the 16-byte grid the bulk
             // copies need: such calls take the plain kernel
@@ -1159,9 +1176,11 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
         const bool prof = plan->prof_used < plan->prof_max;
         const size_t ev = 2 * ((size_t)plan->prof_used * np + i);
         if (prof) CK(cudaEventRecord(plan->prof_ev[ev], st));
-        cudaError_t e = tma                  ? r.ti.fn(p, r.nblocks, st)
-                        : r.kind == PK_PLANE ? r.pi.fn(p, r.nblocks, st)
-                                             : r.li.fn(p, (p.nlines + r.li.nl - 1) / r.li.nl, st);
+        cudaError_t e;
+        if (r.kind == PK_PLANE)
+            e = tma ? r.pti.fn(p, r.plane_tma_blocks, st) : r.pi.fn(p, r.nblocks, st);
+        else
+            e = tma ? r.ti.fn(p, r.nblocks, st) : r.li.fn(p, (p.nlines + r.li.nl - 1) / r.li.nl, st);
         if (e != cudaSuccess) {
             set_error(std::string("kernel launch failed (") + r.note + "): " + cudaGetErrorString(e));
             return RK_ERR_CUDA;
