@@ -215,14 +215,16 @@ __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, 
     return v;
 }
 
-// W_{tw4N}^(e) for e < tw4N via the two-level 2^24 table
+// W_{tw4N}^(e) for e < tw4N via the two-level 2^24 table, formed in FP64 from the
+// FP64 tables and rounded once to the pass precision
 template <typename T>
 __device__ __forceinline__ cplx<T> tw4(const PassParams& p, int64_t e) {
     using V = cplx<T>;
     const int64_t k = (e & (p.tw4_N - 1)) * ((int64_t)1 << TW4_LOG) / p.tw4_N;
-    const V hi = reinterpret_cast<const V*>(p.tw4_hi)[k >> 12];
-    const V lo = reinterpret_cast<const V*>(p.tw4_lo)[k & (TW4_HALF - 1)];
-    return cmul(hi, lo);
+    const double2 hi = __ldg(reinterpret_cast<const double2*>(p.tw4_hi) + (k >> 12));
+    const double2 lo = __ldg(reinterpret_cast<const double2*>(p.tw4_lo) + (k & (TW4_HALF - 1)));
+    const double2 w = cmul(hi, lo);
+    return cmk<V>((T)w.x, (T)w.y);
 }
 
 template <typename T>
@@ -351,28 +353,34 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
             return pos * NL + ln;
     }
 
-    // v[m] *= W_{L/P}^(j1 m), 1 <= m < R, read from the stage table laid out
-    // [m - 1][j1] (TwLayout): every factor is an FP64 value rounded once.
-    template <int R, int J> static __device__ __forceinline__ void twiddle(V* v, int j1, const V* tws) {
-#pragma unroll
-        for (int m = 1; m < R; ++m) v[m] = cmul(v[m], __ldg(tws + (m - 1) * J + j1));
-    }
-
     template <int S, int P>
     static __device__ __forceinline__ void stages(V* v, V* sm, int ln, int tb, const V* tw) {
         if constexpr (S < NS) {
             constexpr int R = RC::R[S];
             constexpr int NB = RT / R;
-#pragma unroll
-            for (int z = 0; z < NB; ++z) dft<R>(v + z * R);
             if constexpr (S + 1 < NS) {
+                // twiddles W_{L/P}^(j1 m), 1 <= m < R, from the stage table laid out
+                // [m - 1][j1] (TwLayout; each an FP64 value rounded once), loaded
+                // before the butterfly so their latency overlaps its arithmetic
                 constexpr int J = L / (P * R);
                 const V* tws = tw + TwLayout<T, L>::offset(S);
 #pragma unroll
                 for (int z = 0; z < NB; ++z) {
                     const int b = tb + TPL * z;
                     const int l = b % P, j1 = b / P;
-                    twiddle<R, J>(v + z * R, j1, tws);
+                    if constexpr (R <= 16) {
+                        V w[R - 1];
+#pragma unroll
+                        for (int m = 1; m < R; ++m) w[m - 1] = __ldg(tws + (m - 1) * J + j1);
+                        dft<R>(v + z * R);
+#pragma unroll
+                        for (int m = 1; m < R; ++m) v[z * R + m] = cmul(v[z * R + m], w[m - 1]);
+                    } else {
+                        // radix 32: keep the register budget, load after the butterfly
+                        dft<R>(v + z * R);
+#pragma unroll
+                        for (int m = 1; m < R; ++m) v[z * R + m] = cmul(v[z * R + m], __ldg(tws + (m - 1) * J + j1));
+                    }
 #pragma unroll
                     for (int m = 0; m < R; ++m) sm[sidx(ln, l + P * (m + R * j1))] = v[z * R + m];
                 }
@@ -385,6 +393,9 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
                     for (int m = 0; m < R2; ++m) v[z * R2 + m] = sm[sidx(ln, tb + TPL * z + (L / R2) * m)];
                 __syncthreads();
                 stages<S + 1, P * R>(v, sm, ln, tb, tw);
+            } else {
+#pragma unroll
+                for (int z = 0; z < NB; ++z) dft<R>(v + z * R);
             }
         }
     }

@@ -936,8 +936,8 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
                 pp.tw2 = (const float2*)tabs->stw_f + tabs->off_f[lg2];
             }
         }
-        pp.tw4_hi = dbl ? tabs->tw4hi_d : tabs->tw4hi_f;
-        pp.tw4_lo = dbl ? tabs->tw4lo_d : tabs->tw4lo_f;
+        pp.tw4_hi = tabs->tw4hi_d;  // FP64 for both precisions (tw4() rounds once)
+        pp.tw4_lo = tabs->tw4lo_d;
         pp.tw4_N = ps.tw4_N;
         pp.status = tabs->status;
         r.L1 = ps.L1;

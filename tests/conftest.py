@@ -35,9 +35,10 @@ def pytest_collection_modifyitems(config, items):
 
 @pytest.fixture
 def rng(request):
-    # seeded per test for reproducibility
-    seed = abs(hash(request.node.nodeid)) % (2**32)
-    return numpy.random.default_rng(seed)
+    # seeded per test from its id, identically in every process
+    import zlib
+
+    return numpy.random.default_rng(zlib.crc32(request.node.nodeid.encode()))
 
 
 @pytest.fixture(scope="session")
