@@ -162,6 +162,22 @@ RK_API int rk_fftshift_execute(void* out, const void* in, int32_t elem_bytes, in
                         const int64_t* shape, int32_t naxes, const int32_t* axes,
                         int32_t inverse, void* scratch, void* stream);
 
+/*
+ * Allocation-free batched 1-D complex64 FFT.  No counterpart in the reference: it
+ * exists for callers that cannot allocate device memory when they need a transform
+ * (code inside a memory pool or arena that owns the device, loops that must not
+ * enter the allocator, hosts that only lend their own buffers).  out/in: contiguous
+ * (batch, n) complex64 device arrays (may alias); n a power of two in
+ * [4096, 1048576]; batch * n <= 4194304 (the 32 MiB static scratch every device that
+ * loads the library holds until exit).  inverse = 1 gives the 1/n-normalised inverse.
+ * Calls no allocating routine.  All calls on a device share the scratch: calls that
+ * may overlap on the GPU race.  The first call on a device resolves the static
+ * arrays and fills its twiddle tables (kernel launches plus a device
+ * synchronisation): make it before any stream capture.  Larger sizes are rejected
+ * with RK_ERR_INVALID.
+ */
+RK_API int rk_fft1d_c64_noalloc(void* out, const void* in, int64_t n, int64_t batch, int32_t inverse, void* stream);
+
 RK_API const char* rk_last_error(void);
 
 /* Library version string. */

@@ -56,6 +56,7 @@ EXPORTED = (
     "rk_fft_profile",
     "rk_fft_profile_read",
     "rk_device_status",
+    "rk_fft1d_c64_noalloc",
 )
 
 I64A = ctypes.c_int64 * MAXD
@@ -170,6 +171,7 @@ def lib() -> ctypes.CDLL:
         L.rk_abi_sizes.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
         L.rk_fft_profile.argtypes = [vp, ctypes.c_int32]
         L.rk_device_status.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
+        L.rk_fft1d_c64_noalloc.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, vp]
         L.rk_fft_profile_read.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
         L.rk_last_error.restype = ctypes.c_char_p
         L.rk_version.restype = ctypes.c_char_p
