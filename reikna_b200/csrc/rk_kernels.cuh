@@ -304,6 +304,47 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
         }
+    } else if (f & SF_FAST2) {
+        // pass-dtype side with an index map a = c cA + j jB (four-step, Bluestein
+        // padding): one line pointer, 32-bit offsets, a bounds predicate, and the
+        // chirp / table ops in side_load's order
+        const int a0 = (int)(la.c * s.cA), jB = (int)s.jB, st = (int)s.ax_stride;
+        const int bound = (int)s.ax_bound, alen = (int)s.ax_len;
+        const V* lp = reinterpret_cast<const V*>(s.ptr) + la.base;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const int a = a0 + pos(i) * jB;
+            v[i] = (la.ok && a < bound) ? lp[a * st] : cmk<V>(T(0), T(0));
+        }
+        if (f & SF_SCALE) {
+            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
+        }
+        if (f & SF_PRE_CONJ) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
+        }
+        if (f & SF_CHIRP) {
+            const V* ch = reinterpret_cast<const V*>(s.chirp);
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int a = a0 + pos(i) * jB;
+                if (a < alen) v[i] = cmul(v[i], __ldg(ch + a));
+            }
+        }
+        if (f & SF_TAB) {
+            const V* tb = reinterpret_cast<const V*>(s.tab);
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int a = a0 + pos(i) * jB;
+                if (a < alen) v[i] = cmul(v[i], __ldg(tb + a));
+            }
+        }
+        if (f & SF_POST_CONJ) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
+        }
     } else {
 #pragma unroll
         for (int i = 0; i < N; ++i) v[i] = side_load<T>(s, la, pos(i));
@@ -330,6 +371,42 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
             const int st = (int)s.ax_stride, sh = s.ax_shift, mask = (int)s.ax_len - 1;
 #pragma unroll
             for (int i = 0; i < N; ++i) lp[((pos(i) + sh) & mask) * st] = v[i];
+        }
+    } else if (f & SF_FAST2) {
+        const int a0 = (int)(la.c * s.cA), jB = (int)s.jB, st = (int)s.ax_stride;
+        const int bound = (int)s.ax_bound, alen = (int)s.ax_len;
+        if (f & SF_TW4) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], tw4<T>(p, la.c * pos(i)));
+        }
+        if (f & SF_PRE_CONJ) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
+        }
+        if (f & SF_CHIRP) {
+            const V* ch = reinterpret_cast<const V*>(s.chirp);
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int a = a0 + pos(i) * jB;
+                if (a < alen) v[i] = cmul(v[i], __ldg(ch + a));
+            }
+        }
+        if (f & SF_POST_CONJ) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
+        }
+        if (f & SF_SCALE) {
+            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
+        }
+        if (la.ok) {
+            V* lp = reinterpret_cast<V*>(s.ptr) + la.base;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int a = a0 + pos(i) * jB;
+                if (a < bound) lp[a * st] = v[i];
+            }
         }
     } else {
 #pragma unroll
@@ -472,11 +549,9 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassPara
         const int p0 = tid / NL;
         const int64_t sline = (int64_t)blockIdx.x * NL + lane;
         const LineAddr la = line_addr(p.st, sline, p.C, p.I, sline < p.nlines);
-#pragma unroll 4
-        for (int q = 0; q < RT; ++q) {
-            const int pos = p0 + TPL * q;
-            side_store<T>(p.st, p, la, pos, sm[E::sidx(lane, pos)]);
-        }
+#pragma unroll
+        for (int q = 0; q < RT; ++q) v[q] = sm[E::sidx(lane, p0 + TPL * q)];
+        store_block<T, RT>(p.st, p, la, [&](int q) { return p0 + TPL * q; }, v);
     } else {
         const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
         store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);

@@ -606,6 +606,19 @@ static void setup_tma(PassRec& r, int dbl, int nsm) {
     r.use_tma = true;
 }
 
+// Sides that cannot take SF_FAST but are still the pass dtype without an index remap
+// (four-step index maps, Bluestein padding, chirp / table ops) take SF_FAST2.
+static void mark_fast2(Side& s, int dbl, int64_t L, int64_t C) {
+    if (s.flags & SF_FAST) return;
+    const int fmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
+    if (s.fmt != fmt || s.ax_shift != 0 || (s.flags & (SF_WINDOW | SF_NORM))) return;
+    if (s.cA < 0 || s.jB < 0 || s.ax_stride < 0) return;
+    const int64_t amax = (C - 1) * s.cA + (L - 1) * s.jB;
+    const int64_t lim = int64_t(1) << 31;
+    if (amax >= lim || s.ax_len >= lim || amax * std::max<int64_t>(s.ax_stride, 1) >= lim) return;
+    s.flags |= SF_FAST2;
+}
+
 static int validate(const rk_fft_desc* d) {
     if (!d) { set_error("null descriptor"); return RK_ERR_INVALID; }
     if (d->dtype != RK_FMT_C64 && d->dtype != RK_FMT_C128) {
@@ -916,6 +929,8 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         build_side(*desc, ps.st, ps.kind == PK_PLANE ? ps.axis2 : ps.axis, dbl, false, pp.st);
         mark_fast(pp.ld, dbl, ps.kind == PK_PLANE ? ps.L2 : ps.L);
         mark_fast(pp.st, dbl, ps.kind == PK_PLANE ? ps.L1 : ps.L);
+        mark_fast2(pp.ld, dbl, ps.kind == PK_PLANE ? ps.L2 : ps.L, ps.C);
+        mark_fast2(pp.st, dbl, ps.kind == PK_PLANE ? ps.L1 : ps.L, ps.C);
         if (!r.ld_edge) pp.ld.ptr = bufs[ps.ld.buf];
         if (!r.st_edge) pp.st.ptr = bufs[ps.st.buf];
         if (ps.ld.chirp_axis >= 0) {
