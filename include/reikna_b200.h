@@ -178,6 +178,28 @@ RK_API int rk_fftshift_execute(void* out, const void* in, int32_t elem_bytes, in
  */
 RK_API int rk_fft1d_c64_noalloc(void* out, const void* in, int64_t n, int64_t batch, int32_t inverse, void* stream);
 
+/*
+ * Batched launch: several plans (any lengths, axes, transformations) executed by one
+ * persistent kernel launch.  The reference runs each compiled computation as its own
+ * chain of kernel launches (ComputationCallable.__call__, reikna/core/computation.py:766);
+ * a batch replaces N such calls.  Every pass of every member must be a line pass with
+ * a compiled batched variant (complex64, power-of-two lengths up to 8192; no plane
+ * passes: plan the members with RK_FLAG_NO_PLANE), else RK_ERR_UNSUPPORTED.  A plan
+ * may appear once per batch.  The batch keeps pointers to the plans: destroy it
+ * before them.  Calls of one batch must be stream-ordered (one stream, or ordered by
+ * the caller); each call waits for the host staging slot it reuses (4 in flight).
+ */
+typedef struct rk_batch rk_batch;
+RK_API int rk_batch_create(rk_fft_plan* const* plans, int32_t nplans, rk_batch** batch);
+/* outputs[i] / inputs[i]: the pointer arrays of member i, as for rk_fft_execute;
+ * inverse, scalars, n_scalars: per member, each may be NULL (forward, no scalars). */
+RK_API int rk_batch_execute(rk_batch* batch, void* const* const* outputs, const void* const* const* inputs,
+                            const int32_t* inverse, const double* const* scalars, const int32_t* n_scalars,
+                            void* stream);
+RK_API int rk_batch_destroy(rk_batch* batch);
+/* tiles (tasks), passes and grid size of the persistent launch */
+RK_API int rk_batch_info(const rk_batch* batch, int64_t* ntasks, int32_t* npasses, int32_t* grid);
+
 RK_API const char* rk_last_error(void);
 
 /* Library version string. */

@@ -57,6 +57,10 @@ EXPORTED = (
     "rk_fft_profile_read",
     "rk_device_status",
     "rk_fft1d_c64_noalloc",
+    "rk_batch_create",
+    "rk_batch_execute",
+    "rk_batch_destroy",
+    "rk_batch_info",
 )
 
 I64A = ctypes.c_int64 * MAXD
@@ -173,6 +177,11 @@ def lib() -> ctypes.CDLL:
         L.rk_device_status.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
         L.rk_fft1d_c64_noalloc.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, vp]
         L.rk_fft_profile_read.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+        i32p, i64p = ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)
+        L.rk_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(vp)]
+        L.rk_batch_execute.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), i32p, ctypes.POINTER(vp), i32p, vp]
+        L.rk_batch_destroy.argtypes = [vp]
+        L.rk_batch_info.argtypes = [vp, i64p, i32p, i32p]
         L.rk_last_error.restype = ctypes.c_char_p
         L.rk_version.restype = ctypes.c_char_p
         for name in EXPORTED:
@@ -279,6 +288,68 @@ class Plan:
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             lib().rk_fft_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+
+def device_status(clear: bool = False) -> int:
+    """Device status word of the current device (nonzero: a kernel gave up a bounded
+    wait or met a task it has no code for); synchronises the device."""
+    v = ctypes.c_int32(0)
+    check(lib().rk_device_status(ctypes.byref(v), int(bool(clear))))
+    return int(v.value)
+
+
+class Batch:
+    """Owns an ``rk_batch``: several plans run by one persistent kernel launch."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)  # the batch points into the plans: keep them alive
+        arr = (ctypes.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
+        h = ctypes.c_void_p()
+        check(lib().rk_batch_create(arr, len(self.plans), ctypes.byref(h)))
+        self._h = h
+
+    def info(self) -> dict:
+        nt, npass, grid = ctypes.c_int64(0), ctypes.c_int32(0), ctypes.c_int32(0)
+        check(lib().rk_batch_info(self._h, ctypes.byref(nt), ctypes.byref(npass), ctypes.byref(grid)))
+        return {"tasks": int(nt.value), "passes": int(npass.value), "grid": int(grid.value)}
+
+    def execute(self, calls, stream: int = 0) -> None:
+        """``calls[i] = (outs, ins, inverse, scalars)`` for member i."""
+        n = len(self.plans)
+        if len(calls) != n:
+            raise ValueError(f"batch has {n} members, got {len(calls)} calls")
+        keep = []
+        outs_a = (ctypes.c_void_p * n)()
+        ins_a = (ctypes.c_void_p * n)()
+        inv_a = (ctypes.c_int32 * n)()
+        sc_a = (ctypes.c_void_p * n)()
+        nsc_a = (ctypes.c_int32 * n)()
+        for i, (outs, ins, inverse, scalars) in enumerate(calls):
+            o = (ctypes.c_void_p * len(outs))(*outs)
+            s = (ctypes.c_void_p * len(ins))(*ins)
+            flat = []
+            for v in scalars:
+                c = complex(v)
+                flat += [c.real, c.imag]
+            d = (ctypes.c_double * max(1, len(flat)))(*flat)
+            keep += [o, s, d]
+            outs_a[i] = ctypes.cast(o, ctypes.c_void_p)
+            ins_a[i] = ctypes.cast(s, ctypes.c_void_p)
+            inv_a[i] = int(inverse)
+            sc_a[i] = ctypes.cast(d, ctypes.c_void_p)
+            nsc_a[i] = len(scalars)
+        check(lib().rk_batch_execute(self._h, outs_a, ins_a, inv_a, sc_a, nsc_a, ctypes.c_void_p(stream)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().rk_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -11,6 +11,7 @@ namespace rk {
 
 constexpr uint32_t RK_WAIT_LIMIT = 1u << 26;
 constexpr int32_t RK_STATUS_TIMEOUT = 1;
+constexpr int32_t RK_STATUS_BAD_VARIANT = 2;   // batched task with no compiled tile body
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));

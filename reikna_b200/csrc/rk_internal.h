@@ -57,6 +57,7 @@ struct PassRec {
     int kind = PK_LINE;
     int dbl = 0;
     int L = 0, mode = 0;
+    int var = 0;                   // 0 plain, 1 fused Bluestein, 2 transposed store
     bool blue = false;
     int L1 = 0, L2 = 0;            // plane
     int axis = -1, axis2 = -1;

@@ -495,21 +495,21 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
 // VAR 0: plain pass; VAR 1: fused Bluestein convolution; VAR 2: position-mode
 // compute with a lane-fastest store through shared memory (four-step second pass,
 // whose output positions are strided by N1 while consecutive lines are adjacent).
+// One CTA's tile (NL lines starting at line block * NL) of a line pass; shared by
+// the per-pass kernel k_line and the persistent batch kernel (rk_batch.cu).
 template <typename T, int L, int MODE, int VAR>
-__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassParams p) {
+__device__ __forceinline__ void line_body(const PassParams& p, int64_t block, unsigned char* smem, int tid) {
     using V = cplx<T>;
     using E = Engine<T, L, MODE>;
     using Cfg = LineCfg<T, L, MODE>;
     constexpr int RT = Cfg::RT, TPL = Cfg::TPL, NL = Cfg::NL;
     constexpr int R0 = E::R0, RL = E::RL;
-    extern __shared__ __align__(16) unsigned char rk_smem[];
-    V* sm = reinterpret_cast<V*>(rk_smem);
+    V* sm = reinterpret_cast<V*>(smem);
     const V* tw = reinterpret_cast<const V*>(p.tw);
 
-    const int tid = threadIdx.x;
     const int ln = MODE == MODE_POS ? tid / TPL : tid % NL;
     const int tb = MODE == MODE_POS ? tid % TPL : tid / NL;
-    const int64_t line = (int64_t)blockIdx.x * NL + ln;
+    const int64_t line = block * NL + ln;
     const bool lok = line < p.nlines;
 
     V v[RT];
@@ -547,7 +547,7 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassPara
         // thread t stores lane t % NL, positions t / NL + TPL * q
         const int lane = tid % NL;
         const int p0 = tid / NL;
-        const int64_t sline = (int64_t)blockIdx.x * NL + lane;
+        const int64_t sline = block * NL + lane;
         const LineAddr la = line_addr(p.st, sline, p.C, p.I, sline < p.nlines);
 #pragma unroll
         for (int q = 0; q < RT; ++q) v[q] = sm[E::sidx(lane, p0 + TPL * q)];
@@ -556,6 +556,12 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassPara
         const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
         store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
     }
+}
+
+template <typename T, int L, int MODE, int VAR>
+__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassParams p) {
+    extern __shared__ __align__(16) unsigned char rk_smem[];
+    line_body<T, L, MODE, VAR>(p, blockIdx.x, rk_smem, threadIdx.x);
 }
 
 }  // namespace rk

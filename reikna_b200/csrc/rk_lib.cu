@@ -914,6 +914,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         r.L = ps.L;
         r.mode = ps.mode;
         r.blue = ps.var == 1;
+        r.var = ps.var;
         r.axis = ps.axis;
         r.ld_buf = ps.ld.buf == SB_IN ? BUF_IN : ps.ld.buf == SB_OUT ? BUF_OUT : ps.ld.buf;
         r.st_buf = ps.st.buf == SB_IN ? BUF_IN : ps.st.buf == SB_OUT ? BUF_OUT : ps.st.buf;
@@ -1094,8 +1095,17 @@ static void apply_edge_scale(const rk_edge& e, const double* scalars, int32_t n_
     }
 }
 
-int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
-                   int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars, void* stream) {
+}  // extern "C"
+
+namespace rk {
+
+// Per-call launch parameters of every pass of a plan: user pointers, runtime scale,
+// inverse conjugations; `tma` says whether the pass may take its TMA kernel for this
+// call.  Stages a private copy of the input when an in-place call meets a remapping
+// single-pass plan.  Shared by rk_fft_execute and the batched launch.
+int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
+                      int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars, cudaStream_t st,
+                      std::vector<PassParams>& out, std::vector<char>* tma_ok) {
     if (!plan) { set_error("null plan"); return RK_ERR_INVALID; }
     const rk_fft_desc& d = plan->desc;
     const int need_in = fmt_is_pair(d.input.format) ? 2 : 1;
@@ -1108,7 +1118,6 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
         if (!inputs[i]) { set_error("null input pointer"); return RK_ERR_INVALID; }
     for (int i = 0; i < need_out; ++i)
         if (!outputs[i]) { set_error("null output pointer"); return RK_ERR_INVALID; }
-    cudaStream_t st = (cudaStream_t)stream;
     const void* in0 = inputs[0];
     const void* in1 = need_in > 1 ? inputs[1] : nullptr;
 
@@ -1188,14 +1197,36 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
             if (i == np - 1) p.st.flags ^= SF_POST_CONJ;
         }
         if (r.st_edge && d.output.conj) p.st.flags ^= SF_POST_CONJ;
+        out.push_back(p);
+        if (tma_ok) tma_ok->push_back(tma ? 1 : 0);
+    }
+    return RK_OK;
+}
+
+}  // namespace rk
+
+extern "C" {
+
+int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
+                   int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars, void* stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<PassParams> prm;
+    std::vector<char> tma;
+    prm.reserve(4);
+    int rc = build_call_params(plan, outputs, n_outputs, inputs, n_inputs, inverse, scalars, n_scalars, st, prm, &tma);
+    if (rc) return rc;
+    const size_t np = plan->passes.size();
+    for (size_t i = 0; i < np; ++i) {
+        const PassRec& r = plan->passes[i];
+        const PassParams& p = prm[i];
         const bool prof = plan->prof_used < plan->prof_max;
         const size_t ev = 2 * ((size_t)plan->prof_used * np + i);
         if (prof) CK(cudaEventRecord(plan->prof_ev[ev], st));
         cudaError_t e;
         if (r.kind == PK_PLANE)
-            e = tma ? r.pti.fn(p, r.plane_tma_blocks, st) : r.pi.fn(p, r.nblocks, st);
+            e = tma[i] ? r.pti.fn(p, r.plane_tma_blocks, st) : r.pi.fn(p, r.nblocks, st);
         else
-            e = tma ? r.ti.fn(p, r.nblocks, st) : r.li.fn(p, (p.nlines + r.li.nl - 1) / r.li.nl, st);
+            e = tma[i] ? r.ti.fn(p, r.nblocks, st) : r.li.fn(p, (p.nlines + r.li.nl - 1) / r.li.nl, st);
         if (e != cudaSuccess) {
             set_error(std::string("kernel launch failed (") + r.note + "): " + cudaGetErrorString(e));
             return RK_ERR_CUDA;

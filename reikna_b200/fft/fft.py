@@ -81,12 +81,19 @@ class FFT(Computation):
         plan = N.Plan(d)
         ann = {p.name: p.annotation for p in self._tr_tree.get_leaf_parameters()}
 
-        def runner(stream: int, args):
+        def bind(args):
+            """(output pointers, input pointers, inverse, scalars) of one call."""
             outs = [array_pointer(args[n], ann[n]) for n in ospec.arrays]
             ins = [array_pointer(args[n], ann[n]) for n in ispec.arrays]
             scalars = [scalar_value(args[n]) for n in scalar_names]
-            plan.execute(outs, ins, inverse=int(args["inverse"]), scalars=scalars, stream=stream)
+            return outs, ins, int(args["inverse"]), scalars
+
+        def runner(stream: int, args):
+            outs, ins, inverse, scalars = bind(args)
+            plan.execute(outs, ins, inverse=inverse, scalars=scalars, stream=stream)
 
         runner.launches = plan.launches
         runner.plan = plan
+        runner.bind = bind
+        runner.flags = flags
         return runner
