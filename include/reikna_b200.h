@@ -183,7 +183,8 @@ RK_API int rk_fft1d_c64_noalloc(void* out, const void* in, int64_t n, int64_t ba
  * persistent kernel launch.  The reference runs each compiled computation as its own
  * chain of kernel launches (ComputationCallable.__call__, reikna/core/computation.py:766);
  * a batch replaces N such calls.  Every pass of every member must be a line pass with
- * a compiled batched variant (complex64, power-of-two lengths up to 8192; no plane
+ * a compiled batched variant (complex64; power-of-two lengths up to 8192 along the
+ * contiguous axis, 16 to 256 along strided axes; no plane
  * passes: plan the members with RK_FLAG_NO_PLANE), else RK_ERR_UNSUPPORTED.  A plan
  * may appear once per batch.  The batch keeps pointers to the plans: destroy it
  * before them.  Calls of one batch must be stream-ordered (one stream, or ordered by

@@ -83,8 +83,6 @@ __device__ bool batch_dispatch(int v, const PassParams* p, int64_t block, unsign
         RK_BV(float, 64, MODE_LANE, 0)
         RK_BV(float, 128, MODE_LANE, 0)
         RK_BV(float, 256, MODE_LANE, 0)
-        RK_BV(float, 512, MODE_LANE, 0)
-        RK_BV(float, 1024, MODE_LANE, 0)
         RK_BV(float, 64, MODE_POS, 1)
         RK_BV(float, 128, MODE_POS, 1)
         RK_BV(float, 256, MODE_POS, 1)
@@ -96,8 +94,6 @@ __device__ bool batch_dispatch(int v, const PassParams* p, int64_t block, unsign
         RK_BV(float, 64, MODE_LANE, 1)
         RK_BV(float, 128, MODE_LANE, 1)
         RK_BV(float, 256, MODE_LANE, 1)
-        RK_BV(float, 512, MODE_LANE, 1)
-        RK_BV(float, 1024, MODE_LANE, 1)
         RK_BV(float, 16, MODE_POS, 2)
         RK_BV(float, 32, MODE_POS, 2)
         RK_BV(float, 64, MODE_POS, 2)
@@ -116,9 +112,9 @@ bool batch_variant(int dbl, int L, int mode, int var, int* out) {
     const int lg = ilog2_b(L);
     bool ok = false;
     if (var == 0 && mode == MODE_POS) ok = L <= 8192;
-    if (var == 0 && mode == MODE_LANE) ok = L >= 16 && L <= 1024;
+    if (var == 0 && mode == MODE_LANE) ok = L >= 16 && L <= 256;
     if (var == 1 && mode == MODE_POS) ok = L >= 64 && L <= 8192;
-    if (var == 1 && mode == MODE_LANE) ok = L >= 64 && L <= 1024;
+    if (var == 1 && mode == MODE_LANE) ok = L >= 64 && L <= 256;
     if (var == 2) ok = mode == MODE_POS && L >= 16 && L <= 1024;
     if (ok) *out = vid(0, var, mode, lg);
     return ok;
@@ -130,37 +126,46 @@ __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long lon
     return v;
 }
 
-__global__ void __launch_bounds__(BATCH_NT, 1) k_batch(const BatchArgs a) {
+// Each CTA holds at most two claimed tasks: the one it runs and the next one, claimed
+// early so that the claim's latency hides behind the tile.  The lowest-index claimed
+// task that is not done is always running (every task it depends on has a lower
+// index, so it is done), hence the CTAs never wait on each other in a cycle.
+// Registers are held to 128 (two CTAs an SM) for every tile body.
+__global__ void __launch_bounds__(BATCH_NT, 2) k_batch(const BatchArgs a) {
     extern __shared__ __align__(16) unsigned char rk_smem[];
-    __shared__ long long s_task;
+    __shared__ __align__(16) PassParams s_prm;
+    __shared__ long long s_task[2];
+    static_assert(sizeof(PassParams) % 16 == 0, "parameter copy moves 16-byte words");
     bool healthy = true;
-    for (;;) {
-        if (threadIdx.x == 0) s_task = (long long)atomicAdd(a.next, 1ull);
-        __syncthreads();
-        const long long t = s_task;
-        __syncthreads();
+    if (threadIdx.x == 0) s_task[0] = (long long)atomicAdd(a.next, 1ull);
+    __syncthreads();
+    for (int cur = 0;; cur ^= 1) {
+        const long long t = s_task[cur];
         if (t >= a.ntasks) break;
+        if (threadIdx.x == 0) s_task[cur ^ 1] = (long long)atomicAdd(a.next, 1ull);
         const BatchTask tk = a.tasks[t];
         const BatchPass* bp = a.passes + tk.pass;
+        // the pass parameters go to shared memory: the tile body reads them often
+        const uint4* src = reinterpret_cast<const uint4*>(&bp->prm);
+        uint4* dst = reinterpret_cast<uint4*>(&s_prm);
+        for (int i = threadIdx.x; i < (int)(sizeof(PassParams) / 16); i += BATCH_NT) dst[i] = src[i];
         const int dep = bp->dep;
-        if (dep >= 0) {
-            if (threadIdx.x == 0) {
-                const unsigned long long need = (unsigned long long)a.passes[dep].nblocks;
-                bool ok = ld_acquire(a.done + dep) >= need;
-                if (!ok && healthy) {
-                    const long long t0 = clock64();
-                    while (!(ok = ld_acquire(a.done + dep) >= need))
-                        if (clock64() - t0 > RK_WAIT_CYCLES) break;
-                }
-                if (!ok) {
-                    healthy = false;
-                    atomicOr(a.status, RK_STATUS_TIMEOUT);
-                }
+        if (dep >= 0 && threadIdx.x == 0) {
+            const unsigned long long need = (unsigned long long)a.passes[dep].nblocks;
+            bool ok = ld_acquire(a.done + dep) >= need;
+            if (!ok && healthy) {
+                const long long t0 = clock64();
+                while (!(ok = ld_acquire(a.done + dep) >= need))
+                    if (clock64() - t0 > RK_WAIT_CYCLES) break;
             }
-            __syncthreads();
-            __threadfence();
+            if (!ok) {
+                healthy = false;
+                atomicOr(a.status, RK_STATUS_TIMEOUT);
+            }
         }
-        if (!batch_dispatch(bp->variant, &bp->prm, tk.block, rk_smem) && threadIdx.x == 0)
+        __syncthreads();
+        if (dep >= 0) __threadfence();
+        if (!batch_dispatch(bp->variant, &s_prm, tk.block, rk_smem) && threadIdx.x == 0)
             atomicOr(a.status, RK_STATUS_BAD_VARIANT);
         __syncthreads();
         if (threadIdx.x == 0) {

@@ -36,12 +36,12 @@ RK_RADIX(float, 2, 2, 2)
 RK_RADIX(float, 4, 4, 4)
 RK_RADIX(float, 8, 8, 8)
 RK_RADIX(float, 16, 16, 16)
-RK_RADIX(float, 32, 32, 32)
+RK_RADIX(float, 32, 8, 8, 4)
 RK_RADIX(float, 64, 8, 8, 8)
 RK_RADIX(float, 128, 16, 16, 8)
 RK_RADIX(float, 256, 16, 16, 16)
-RK_RADIX(float, 512, 32, 32, 16)
-RK_RADIX(float, 1024, 32, 32, 32)
+RK_RADIX(float, 512, 16, 16, 16, 2)
+RK_RADIX(float, 1024, 16, 16, 16, 4)
 RK_RADIX(float, 2048, 16, 16, 16, 8)
 RK_RADIX(float, 4096, 16, 16, 16, 16)
 RK_RADIX(float, 8192, 32, 32, 16, 16)
@@ -220,7 +220,9 @@ __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, 
 template <typename T>
 __device__ __forceinline__ cplx<T> tw4(const PassParams& p, int64_t e) {
     using V = cplx<T>;
-    const int64_t k = (e & (p.tw4_N - 1)) * ((int64_t)1 << TW4_LOG) / p.tw4_N;
+    // tw4_N is a power of two <= 2^TW4_LOG: scale the exponent by a shift
+    const int sh = TW4_LOG - (63 - __clzll((unsigned long long)p.tw4_N));
+    const int64_t k = (e & (p.tw4_N - 1)) << sh;
     const double2 hi = __ldg(reinterpret_cast<const double2*>(p.tw4_hi) + (k >> 12));
     const double2 lo = __ldg(reinterpret_cast<const double2*>(p.tw4_lo) + (k & (TW4_HALF - 1)));
     const double2 w = cmul(hi, lo);
@@ -560,6 +562,20 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
 
 template <typename T, int L, int MODE, int VAR>
 __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassParams p) {
+    extern __shared__ __align__(16) unsigned char rk_smem[];
+    line_body<T, L, MODE, VAR>(p, blockIdx.x, rk_smem, threadIdx.x);
+}
+
+// Fused Bluestein bodies with 16 elements a thread would take 160-180 registers;
+// k_line_2 holds them to 128 so that two 256-thread CTAs share an SM.  Other bodies
+// keep the register count ptxas picks by itself (any minimum-blocks bound, 1
+// included, lets it spend registers up to the bound).
+template <typename T, int L, int MODE, int VAR> struct LineMinBlocks {
+    static constexpr int V = (VAR == 1 && Radix<T, L>::RT == 16 && L >= 512 && LineCfg<T, L, MODE>::NT <= 256) ? 2 : 1;
+};
+
+template <typename T, int L, int MODE, int VAR>
+__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT, 2) k_line_2(const PassParams p) {
     extern __shared__ __align__(16) unsigned char rk_smem[];
     line_body<T, L, MODE, VAR>(p, blockIdx.x, rk_smem, threadIdx.x);
 }
