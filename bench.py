@@ -165,12 +165,17 @@ def run_reference(args, rank: int, world: int) -> int:
     threads = os.cpu_count() or 1
     plan = oracle.Plan(SHAPE, (0, 1, 2))
     out = numpy.empty_like(x)
+    tw = time.perf_counter()
     for _ in range(args.warmup):
         plan.shifted(x, scale=1.0 / NTOT, threads=threads, out=out)
+    per = (time.perf_counter() - tw) / max(1, args.warmup)
+    # a step is one full transform on the host cores (about 0.2 s); the run is held to
+    # about two minutes, so at most that many steps of the K requested are timed
+    steps = max(1, min(args.steps, int(120.0 / max(per, 1e-6))))
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         plan.shifted(x, scale=1.0 / NTOT, threads=threads, out=out)
-    t = (time.perf_counter() - t0) / max(1, args.steps)
+    t = (time.perf_counter() - t0) / steps
     value = B_ALG / t / 1e9
     line = {
         "impl": "reference",
@@ -179,6 +184,7 @@ def run_reference(args, rank: int, world: int) -> int:
         "unit": "GB/s",
         "n_gpus": world,
         "steps": args.steps,
+        "steps_timed": steps,
         "warmup": args.warmup,
         "ms_per_step": t * 1e3,
         "higher_is_better": True,
@@ -350,6 +356,198 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
     return 0
 
 
+# --- serving stream ---------------------------------------------------------------
+
+
+def _primes_log_spaced(count: int = 16, lo: int = 61, hi: int = 65521) -> list[int]:
+    """``count`` primes spread log-uniformly over [lo, hi] (the largest prime at or
+    below each log-spaced target)."""
+    import numpy
+
+    sieve = numpy.ones(hi + 1, bool)
+    sieve[:2] = False
+    for k in range(2, int(hi**0.5) + 1):
+        if sieve[k]:
+            sieve[k * k :: k] = False
+    primes = numpy.nonzero(sieve)[0]
+    out = []
+    for t in numpy.geomspace(lo, hi, count):
+        out.append(int(primes[numpy.searchsorted(primes, t, side="right") - 1]))
+    return sorted(set(out))
+
+
+def _p_min(m: int, c_log: int = 14) -> int:
+    import math
+
+    return max(1, math.ceil(math.log2(max(m, 2)) / c_log))
+
+
+def _bpow2(n: int) -> int:
+    return 1 << (n - 1).bit_length()
+
+
+def serve_stream(n: int, seed: int, dev, on_device: bool = False):
+    """Synthetic request stream (seeded): 60% 1-D C2C with N uniform over the powers of
+    two 2^6..2^20 and 16 log-spaced primes in [61, 65521], rows U{1..256}; 20% 2-D C2C
+    with each side a power of two in 2^6..2^11; 20% spectrograms of a 2^22-sample
+    float32 signal (N(0,1) plus 8 sinusoids), Hann window 1024, hop 256.  Inputs are
+    views of shared pinned pools (their contents do not change the work); results go
+    to shared pinned output pools.  Returns (requests, algorithmic bytes per request)."""
+    import numpy
+    import torch
+
+    from reikna_b200.serve import FFTRequest
+    from reikna_b200.spectrogram import frames
+
+    rng = numpy.random.default_rng(seed)
+    lengths = [2**k for k in range(6, 21)] + _primes_log_spaced()
+    cap = 2**20 * 256
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    pool = torch.complex(torch.randn(cap, device=dev, generator=gen), torch.randn(cap, device=dev, generator=gen))
+    if on_device:
+        out_pool = torch.empty(cap, dtype=torch.complex64, device=dev)
+    else:
+        pool = pool.cpu().pin_memory()
+        out_pool = torch.empty(cap, dtype=torch.complex64).pin_memory()
+    slen, nfft, hop = 2**22, 1024, 256
+    t = numpy.arange(slen)
+    sig = rng.standard_normal(slen)
+    for _ in range(8):
+        sig += rng.uniform(0.1, 2) * numpy.sin(2 * numpy.pi * rng.uniform(0, 0.5) * t + rng.uniform(0, 2 * numpy.pi))
+    sig_t = torch.from_numpy(sig.astype(numpy.float32))
+    spec_out = torch.empty((frames(slen, nfft, hop), nfft // 2 + 1), dtype=torch.float32)
+    sig_t, spec_out = (sig_t.to(dev), spec_out.to(dev)) if on_device else (sig_t.pin_memory(), spec_out.pin_memory())
+    reqs, nbytes = [], []
+    for _ in range(n):
+        u = rng.uniform()
+        if u < 0.6:
+            ln = int(rng.choice(lengths))
+            rows = int(rng.integers(1, 257))
+            data = pool[: rows * ln].view(rows, ln)
+            reqs.append(FFTRequest("fft1d", data, out=out_pool[: rows * ln].view(rows, ln)))
+            m = ln if ln & (ln - 1) == 0 else 2 * _bpow2(ln)
+            nbytes.append(_p_min(m) * 2 * rows * ln * 8)
+        elif u < 0.8:
+            n1, n2 = (2 ** int(rng.integers(6, 12)) for _ in range(2))
+            data = pool[: n1 * n2].view(n1, n2)
+            reqs.append(FFTRequest("fft2d", data, out=out_pool[: n1 * n2].view(n1, n2)))
+            nbytes.append(_p_min(n1 * n2) * 2 * n1 * n2 * 8)
+        else:
+            reqs.append(FFTRequest("spectrogram", sig_t, nfft=nfft, hop=hop, out=spec_out))
+            nbytes.append(_p_min(nfft) * (slen * 4 + spec_out.numel() * 4))
+    return reqs, nbytes
+
+
+def _reset(reqs):
+    for r in reqs:
+        r.done = False
+        r.result = None
+        r.arrival = r.launched = r.finished = 0.0
+
+
+def _lat_ms(reqs) -> dict:
+    import numpy
+
+    lat = numpy.array([r.latency for r in reqs]) * 1e3
+    return {"p50": float(numpy.percentile(lat, 50)), "p99": float(numpy.percentile(lat, 99)), "mean": float(lat.mean())}
+
+
+def run_serve(args, rank: int, world: int, local_rank: int) -> int:
+    """Serving stream: continuous-batching server against per-call plain execution."""
+    import numpy
+    import torch
+
+    from reikna_b200.serve import FFTServer, serve_plain
+
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    on_device = args.serve_data == "device"
+    reqs, nbytes = serve_stream(args.requests, 9, dev, on_device)
+    total = float(sum(nbytes))
+    srv = FFTServer(dev, memory_budget=40 << 30, streams=args.streams, depth=2)
+    plain_cache = None
+    import collections
+
+    plain_cache = collections.OrderedDict()
+    # warm pass of each arm: plans compiled and resident
+    t_prep = time.perf_counter()
+    srv.prepare(reqs)
+    t_prep = time.perf_counter() - t_prep
+    srv.run(reqs)
+    _reset(reqs)
+    torch.cuda.empty_cache()
+    serve_plain(reqs, dev, cache=plain_cache)
+    _reset(reqs)
+    torch.cuda.synchronize(dev)
+    warm_compiles = srv.plans.compiles
+    with Clocks(local_rank) as clk:
+        t_srv = srv.run(reqs)
+        _reset(reqs)
+        t_plain = serve_plain(reqs, dev, cache=plain_cache)
+        _reset(reqs)
+        rate = args.load * len(reqs) / t_srv
+        offs = numpy.cumsum(numpy.random.default_rng(10).exponential(1.0 / rate, len(reqs))).tolist()
+        t_srv_p = srv.run(reqs, offs)
+        lat_srv = _lat_ms(reqs)
+        _reset(reqs)
+        t_plain_p = serve_plain(reqs, dev, offsets=offs, cache=plain_cache)
+        lat_plain = _lat_ms(reqs)
+    h2d = sum(r.in_bytes() for r in reqs)
+    d2h = sum(int(numpy.prod(r.out_shape())) * (4 if r.kind == "spectrogram" else 8) for r in reqs)
+    kinds = collections.Counter(r.kind for r in reqs)
+    line = {
+        "metric": METRIC,
+        "value": total / t_srv / 1e9,
+        "unit": "GB/s",
+        "n_gpus": 1,
+        "steps": 1,
+        "warmup": 1,
+        "ms_per_step": t_srv * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": "serve_stream",
+            "requests": len(reqs),
+            "mix": dict(kinds),
+            "memory_budget_bytes": 40 << 30,
+            "streams": args.streams,
+            "data": args.serve_data,
+            "note": "value = algorithmic bytes of all requests / wall time of a burst (all arrive at t=0); "
+            + ("inputs and outputs in device memory" if on_device else "host pinned inputs and outputs, copies included"),
+        },
+        "req_per_s": len(reqs) / t_srv,
+        "plain": {"value": total / t_plain / 1e9, "req_per_s": len(reqs) / t_plain, "s": t_plain},
+        "speedup_vs_plain": t_plain / t_srv,
+        "poisson": {
+            "rate_req_per_s": rate,
+            "load_vs_served_capacity": args.load,
+            "served_latency_ms": lat_srv,
+            "plain_latency_ms": lat_plain,
+            "served_s": t_srv_p,
+            "plain_s": t_plain_p,
+        },
+        "groups": srv.groups,
+        "plans": {
+            "prepared": warm_compiles,
+            "prepare_s": t_prep,
+            "compiled_while_timed": srv.plans.compiles - warm_compiles,
+            "evictions": srv.plans.evictions,
+            "resident_bytes": srv.plans.bytes,
+            "plain_cache_plans": len(plain_cache),
+        },
+        "e2e": {"value": total / t_srv / 1e9, "unit": "GB/s", "h2d_bytes_per_step": 0 if on_device else h2d,
+                "d2h_bytes_per_step": 0 if on_device else d2h},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,6 +555,13 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["own", "reference"], default="own")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["fft3d", "serve"], default="fft3d",
+                    help="fft3d: the headline 256^3 transform; serve: the request stream")
+    ap.add_argument("--requests", type=int, default=1000, help="serve: requests in the stream")
+    ap.add_argument("--streams", type=int, default=4, help="serve: compute streams of the server")
+    ap.add_argument("--load", type=float, default=0.7, help="serve: Poisson rate / served burst rate")
+    ap.add_argument("--serve-data", choices=["host", "device"], default="host",
+                    help="serve: request data in pinned host memory or already in device memory")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
@@ -365,6 +570,8 @@ def main(argv=None) -> int:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "serve":
+        return run_serve(args, rank, world, local_rank)
     return run_own(args, rank, world, local_rank)
 
 
