@@ -69,7 +69,8 @@ extern "C" {
 /* plan flags */
 #define RK_FLAG_NO_PLANE 1   /* never fuse two axes into one clustered pass */
 #define RK_FLAG_NO_BLUE1 2   /* never use the single-pass Bluestein kernel */
-#define RK_FLAG_SPLIT_TC 4   /* tensor-core split-precision radix-16 stages */
+#define RK_FLAG_SPLIT_TC 4   /* tensor-core split-precision radix-16 stages (1024-point
+                                contiguous complex64 line passes; others run as usual) */
 #define RK_FLAG_PLANE_WIDE 8 /* plane pass on twice as many CTAs per cluster (tuning) */
 #define RK_FLAG_NO_TMA 16    /* never use the persistent TMA-fed line passes */
 
@@ -143,6 +144,10 @@ RK_API int rk_fft_plan_describe(const rk_fft_desc* desc, char* buf, int64_t cap,
 
 /* Number of kernels rk_fft_execute launches for this plan. */
 RK_API int rk_fft_plan_launches(const rk_fft_plan* plan, int32_t* n);
+
+/* Number of the plan's passes that run on the tensor cores (RK_FLAG_SPLIT_TC).  No
+ * counterpart in the reference, which has no tensor-core path. */
+RK_API int rk_fft_plan_tc_passes(const rk_fft_plan* plan, int32_t* n);
 
 /* Per-pass timing: record a CUDA event pair around every kernel of the next
  * `max_calls` rk_fft_execute calls (0 stops recording and frees the events).

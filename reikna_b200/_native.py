@@ -61,6 +61,7 @@ EXPORTED = (
     "rk_batch_execute",
     "rk_batch_destroy",
     "rk_batch_info",
+    "rk_fft_plan_tc_passes",
 )
 
 I64A = ctypes.c_int64 * MAXD
@@ -160,6 +161,7 @@ def lib() -> ctypes.CDLL:
             ctypes.POINTER(ctypes.c_int64),
         ]
         L.rk_fft_plan_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+        L.rk_fft_plan_tc_passes.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
         L.rk_fftshift_execute.argtypes = [
             vp,
             vp,
@@ -250,6 +252,13 @@ class Plan:
         n = ctypes.c_int32(0)
         check(lib().rk_fft_plan_launches(h, ctypes.byref(n)))
         self.launches = int(n.value)
+
+    @property
+    def tc_passes(self) -> int:
+        """Passes running on the tensor cores (split-precision mode)."""
+        n = ctypes.c_int32(0)
+        check(lib().rk_fft_plan_tc_passes(self._h, ctypes.byref(n)))
+        return int(n.value)
 
     @property
     def device_bytes(self) -> int:

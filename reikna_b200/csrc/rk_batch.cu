@@ -226,7 +226,7 @@ extern "C" int rk_batch_create(rk_fft_plan* const* plans, int32_t nplans, rk_bat
         maxlevel = std::max<int>(maxlevel, (int)p->passes.size());
         for (const PassRec& r : p->passes) {
             int v = 0;
-            if (r.kind != PK_LINE || !batch_variant(r.dbl, r.L, r.mode, r.var, &v))
+            if (r.kind != PK_LINE || r.use_tc || !batch_variant(r.dbl, r.L, r.mode, r.var, &v))
                 return fail(RK_ERR_UNSUPPORTED, "rk_batch_create: pass '" + r.note + "' (L=" + std::to_string(r.L) +
                                                      ") has no batched variant");
             smem = std::max(smem, r.li.smem);

@@ -74,11 +74,16 @@ struct PassRec {
     bool use_plane_tma = false;
     int64_t plane_tma_blocks = 0;
     bool use_tma = false;
+    bool use_tc = false;           // tensor-core split-precision kernel (RK_FLAG_SPLIT_TC)
     bool tma_reencode = false;     // tensor map over the user's input: re-encode per call
     const void* tma_ptr = nullptr; // pointer the current map was encoded for
     int tma_rows = 0;
     std::string note;
 };
+
+// tensor-core split-precision pass (rk_tc.cu): 1024-point complex64 contiguous lines
+bool tc_eligible(const PassRec& r);
+cudaError_t tc_launch(const PassParams& p, int64_t nblocks, cudaStream_t st);
 
 struct DeviceTables {
     void* stw_f = nullptr;     // float2 stage twiddle tables, all L (TwLayout)

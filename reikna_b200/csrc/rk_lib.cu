@@ -993,6 +993,10 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             r.nblocks = (pp.nlines + li.nl - 1) / li.nl;
             r.li = li;
             if (!(desc->flags & RK_FLAG_NO_TMA) && ps.var == 0) setup_tma(r, dbl, nsm);
+            if ((desc->flags & RK_FLAG_SPLIT_TC) && tc_eligible(r)) {
+                r.use_tc = true;
+                r.use_tma = false;
+            }
         }
         plan->passes.push_back(r);
     }
@@ -1073,6 +1077,14 @@ int rk_fft_plan_device_bytes(const rk_fft_plan* plan, int64_t* bytes) {
 int rk_fft_plan_launches(const rk_fft_plan* plan, int32_t* n) {
     if (!plan || !n) { set_error("null argument"); return RK_ERR_INVALID; }
     *n = (int32_t)plan->passes.size();
+    return RK_OK;
+}
+
+int rk_fft_plan_tc_passes(const rk_fft_plan* plan, int32_t* n) {
+    if (!plan || !n) { set_error("null argument"); return RK_ERR_INVALID; }
+    int32_t k = 0;
+    for (const PassRec& r : plan->passes) k += r.use_tc ? 1 : 0;
+    *n = k;
     return RK_OK;
 }
 
@@ -1225,6 +1237,8 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
         cudaError_t e;
         if (r.kind == PK_PLANE)
             e = tma[i] ? r.pti.fn(p, r.plane_tma_blocks, st) : r.pi.fn(p, r.nblocks, st);
+        else if (r.use_tc)
+            e = tc_launch(p, r.nblocks, st);
         else
             e = tma[i] ? r.ti.fn(p, r.nblocks, st) : r.li.fn(p, (p.nlines + r.li.nl - 1) / r.li.nl, st);
         if (e != cudaSuccess) {

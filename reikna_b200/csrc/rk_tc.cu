@@ -1,0 +1,322 @@
+// Tensor-core split-precision line pass for 1024-point complex64 transforms along a
+// contiguous axis (the precision mode, RK_FLAG_SPLIT_TC).
+//
+// A 1024-point DFT is taken as 16 x 16 x 4: two radix-16 stages on the tensor cores
+// and a radix-4 stage on the CUDA cores.  A radix-16 DFT of 128 vectors is one
+// 128 x 32 x 32 real matrix product: the rows are the vectors (real parts then
+// imaginary parts, K = 32), the 32 x 32 matrix is the real form of the 16-point DFT
+// matrix, and the 32 output columns are the real and imaginary parts of the result.
+//
+// Precision: every operand is split as hi + lo with hi = fp16(v) and lo = fp16(v -
+// hi), which keeps about 22 significant bits; the product is hi*hi + lo*hi + hi*lo
+// accumulated in FP32 in tensor memory (lo*lo is below FP32 rounding of the sum).
+// Each vector is first scaled by a power of two that brings its largest component to
+// [2^14, 2^15), so fp16's range holds it, and the result is scaled back exactly.
+// Twiddles are FP64-generated and rounded once to FP32; they and the radix-4 stage
+// run in FP32 on the CUDA cores.
+//
+// Per tile of two lines (2048 points) the CTA's 128 threads each own one row of the
+// matrix product: they convert their vector into the hi / lo operand tiles (the
+// no-swizzle K-major canonical layout of the UMMA shared-memory descriptor), one
+// elected thread issues the six tcgen05.mma of a stage and commits them to an
+// mbarrier, and every thread reads its row of the FP32 accumulator back from tensor
+// memory with tcgen05.ld.  The grid is persistent; tensor memory (32 columns) is
+// allocated once per CTA and freed before exit, also after a timed-out wait.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "rk_async.cuh"
+#include "rk_internal.h"
+#include "rk_kernels.cuh"
+
+namespace rk {
+
+namespace {
+
+constexpr int TC_NT = 128;     // threads = rows of one matrix product
+constexpr int TC_L = 1024;
+constexpr int TC_LINES = 2;    // lines per tile (2 x 64 vectors of 16 per stage)
+constexpr int TC_XS = 68;      // padded row, in complex elements, of the exchange buffer
+
+struct __align__(128) TcSmem {
+    __half a_hi[TC_NT * 32];   // 8 KB each, canonical K-major layout
+    __half a_lo[TC_NT * 32];
+    __half b_hi[32 * 32];
+    __half b_lo[32 * 32];
+    float2 tw[TC_L];           // W_1024^m
+    float2 x[TC_LINES * 16 * TC_XS];
+    uint64_t bar;
+    uint32_t tmem;
+};
+
+// element (row r, column k) of a 32-column operand in the no-swizzle K-major layout:
+// 8 x 8 core matrices of 128 contiguous bytes, K-adjacent ones 128 bytes apart (LBO),
+// row-adjacent ones 512 bytes apart (SBO)
+__device__ __forceinline__ int op_idx(int r, int k) { return (r >> 3) * 256 + (k >> 3) * 64 + (r & 7) * 8 + (k & 7); }
+
+__device__ __forceinline__ uint64_t smem_desc(const void* p) {
+    const uint64_t addr = smem_u32(p);
+    return ((addr >> 4) & 0x3FFF) | (uint64_t(128 >> 4) << 16) | (uint64_t(512 >> 4) << 32) | (uint64_t(1) << 46);
+}
+
+// kind::f16 instruction descriptor: D f32, A and B f16, both K-major, N = 32, M = 128
+constexpr uint32_t TC_IDESC = (1u << 4) | (0u << 7) | (0u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(TC_IDESC), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// this thread's 32 accumulator columns (its row = its tensor-memory lane)
+__device__ __forceinline__ void tc_ld_row(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// scale the 16-point vector u to [2^14, 2^15) at its largest component, split it into
+// hi / lo fp16 rows of the operand tiles; returns the exponent to undo
+__device__ __forceinline__ int tc_put_row(TcSmem& S, int row, const float2* u) {
+    float m = 0.f;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) m = fmaxf(m, fmaxf(fabsf(u[j].x), fabsf(u[j].y)));
+    const int e = m > 0.f ? 14 - ilogbf(m) : 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        // column chunk c holds k = 8c .. 8c+7: real parts (c < 2) or imaginary parts
+        __align__(16) __half hi[8], lo[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int j = (c & 1) * 8 + i;
+            const float v = ldexpf(c < 2 ? u[j].x : u[j].y, e);
+            hi[i] = __float2half_rn(v);
+            lo[i] = __float2half_rn(v - __half2float(hi[i]));
+        }
+        *reinterpret_cast<uint4*>(&S.a_hi[op_idx(row, 8 * c)]) = *reinterpret_cast<const uint4*>(hi);
+        *reinterpret_cast<uint4*>(&S.a_lo[op_idx(row, 8 * c)]) = *reinterpret_cast<const uint4*>(lo);
+    }
+    return e;
+}
+
+// one radix-16 stage of the 128 rows: split products into tensor memory, then this
+// thread's row back, scaled by 2^-e; false if the wait ran out
+__device__ __forceinline__ bool tc_stage(TcSmem& S, uint32_t tmem, uint32_t& phase, int e, float2* y,
+                                         int32_t* status) {
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tc_fence_after();
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            // K step s covers operand columns 16 s .. 16 s + 15 (two 128-byte chunks)
+            const uint64_t ah = smem_desc(&S.a_hi[s * 128]), al = smem_desc(&S.a_lo[s * 128]);
+            const uint64_t bh = smem_desc(&S.b_hi[s * 128]), bl = smem_desc(&S.b_lo[s * 128]);
+            tc_mma(tmem, ah, bh, s > 0);
+            tc_mma(tmem, al, bh, 1);
+            tc_mma(tmem, ah, bl, 1);
+        }
+        tc_commit(&S.bar);
+    }
+    bool ok = mbar_wait(&S.bar, phase, status);
+    phase ^= 1;
+    // every thread leaves together when any wait ran out
+    ok = __syncthreads_and(ok);
+    if (!ok) return false;
+    tc_fence_after();
+    float v[32];
+    const uint32_t warp = threadIdx.x >> 5;
+    tc_ld_row(tmem + ((warp * 32) << 16), v);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) y[q] = make_float2(ldexpf(v[q], -e), ldexpf(v[16 + q], -e));
+    return true;
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__global__ void __launch_bounds__(TC_NT) k_tc1024(const __grid_constant__ PassParams p) {
+    extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>(tc_smem_raw);
+    const int t = threadIdx.x;
+    const int warp = t >> 5, lane = t & 31;
+
+    // tables: W_1024^m and the real 32 x 32 DFT-16 matrix B[n][k] (K-major) as hi / lo
+    for (int e = t; e < TC_L; e += TC_NT) {
+        double s, c;
+        sincospi(-2.0 * e / TC_L, &s, &c);
+        S.tw[e] = make_float2((float)c, (float)s);
+        const int n = e >> 5, k = e & 31;
+        const int m = ((k & 15) * (n & 15)) & 15;
+        double sv, cv;
+        sincospi(m / 8.0, &sv, &cv);
+        // Y = X W_16^(jq):  Yr = Xr c + Xi s,  Yi = Xi c - Xr s
+        const double v = ((k < 16) == (n < 16)) ? cv : (k < 16 ? -sv : sv);
+        const __half hi = __double2half(v);
+        S.b_hi[op_idx(n, k)] = hi;
+        S.b_lo[op_idx(n, k)] = __double2half(v - (double)__half2float(hi));
+    }
+    if (t == 0) {
+        mbar_init(&S.bar, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(&S.tmem))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+
+    const Side& ld = p.ld;
+    const Side& st = p.st;
+    const bool ld_scale = ld.flags & SF_SCALE, st_scale = st.flags & SF_SCALE;
+    const bool ld_conj = ((ld.flags & SF_PRE_CONJ) != 0) != ((ld.flags & SF_POST_CONJ) != 0);
+    const bool st_conj = ((st.flags & SF_PRE_CONJ) != 0) != ((st.flags & SF_POST_CONJ) != 0);
+    const float2 lsc = make_float2((float)ld.scale_re, (float)ld.scale_im);
+    const float2 ssc = make_float2((float)st.scale_re, (float)st.scale_im);
+    const float2* src = reinterpret_cast<const float2*>(ld.ptr) + ld.offset;
+    float2* dst = reinterpret_cast<float2*>(st.ptr) + st.offset;
+    const int64_t ntiles = (p.nlines + TC_LINES - 1) / TC_LINES;
+    uint32_t phase = 0;
+
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        // ---- stage 1: radix 16 over n1 of n = 64 n1 + n2; row t = (line, n2) ----
+        {
+            const int ll = t >> 6, n2 = t & 63;
+            const int64_t line = tile * TC_LINES + ll;
+            const bool ok = line < p.nlines;
+            float2 u[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                float2 v = ok ? src[line * TC_L + 64 * j + n2] : make_float2(0.f, 0.f);
+                if (ld_scale) v = cmulf(v, lsc);
+                if (ld_conj) v.y = -v.y;
+                u[j] = v;
+            }
+            const int e = tc_put_row(S, t, u);
+            float2 y[16];
+            if (!tc_stage(S, tmem, phase, e, y, p.status)) break;
+            // twiddle W_1024^(n2 k1), then X1[line][k1][n2] to the exchange buffer
+#pragma unroll
+            for (int k1 = 0; k1 < 16; ++k1) S.x[(ll * 16 + k1) * TC_XS + n2] = cmulf(y[k1], S.tw[(n2 * k1) & (TC_L - 1)]);
+        }
+        tc_fence_before();
+        __syncthreads();
+        // ---- stage 2: radix 16 over m1 of n2 = 4 m1 + m2; row t = (line, k1, m2) ----
+        {
+            const int ll = t >> 6, k1 = (t >> 2) & 15, m2 = t & 3;
+            float2 u[16];
+#pragma unroll
+            for (int m1 = 0; m1 < 16; ++m1) u[m1] = S.x[(ll * 16 + k1) * TC_XS + 4 * m1 + m2];
+            const int e = tc_put_row(S, t, u);
+            float2 y[16];
+            if (!tc_stage(S, tmem, phase, e, y, p.status)) break;
+            // twiddle W_64^(m2 q1) = W_1024^(16 m2 q1), then radix 4 over m2 (lanes
+            // 4c .. 4c + 3 hold m2 = 0 .. 3 of the same (line, k1)):
+            //   Z[q1 + 16 q2] = sum_m2 V_m2[q1] (-i)^(m2 q2), this lane computes q2 = m2
+            const int64_t line = tile * TC_LINES + ll;
+            const bool ok = line < p.nlines;
+            const int base = lane & ~3;
+#pragma unroll
+            for (int q1 = 0; q1 < 16; ++q1) {
+                const float2 w = cmulf(y[q1], S.tw[(16 * m2 * q1) & (TC_L - 1)]);
+                float2 v[4];
+#pragma unroll
+                for (int mm = 0; mm < 4; ++mm) {
+                    v[mm].x = __shfl_sync(0xffffffffu, w.x, base + mm);
+                    v[mm].y = __shfl_sync(0xffffffffu, w.y, base + mm);
+                }
+                // (-i)^(mm m2): powers of -i rotate (x, y) -> (y, -x)
+                float2 z = v[0];
+#pragma unroll
+                for (int mm = 1; mm < 4; ++mm) {
+                    const int r = (mm * m2) & 3;
+                    const float2 a = v[mm];
+                    const float2 b = r == 0 ? a : r == 1 ? make_float2(a.y, -a.x) : r == 2 ? make_float2(-a.x, -a.y)
+                                                                                   : make_float2(-a.y, a.x);
+                    z.x += b.x;
+                    z.y += b.y;
+                }
+                if (st_conj) z.y = -z.y;
+                if (st_scale) z = cmulf(z, ssc);
+                if (ok) dst[line * TC_L + k1 + 16 * q1 + 256 * m2] = z;
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    // all tensor-memory reads are done (or abandoned after a timed-out wait)
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+}
+
+}  // namespace
+
+bool tc_eligible(const PassRec& r) {
+    const PassParams& p = r.prm;
+    if (r.dbl || r.kind != PK_LINE || r.L != TC_L || r.mode != MODE_POS || r.var != 0) return false;
+    if (p.C != 1 || p.I != 1) return false;
+    for (const Side* s : {&p.ld, &p.st}) {
+        if (!(s->flags & SF_FAST) || s->ax_stride != 1 || s->ax_shift != 0 || s->nd_i != 0) return false;
+        if (s->flags & ~(SF_FAST | SF_FAST2 | SF_SCALE | SF_PRE_CONJ | SF_POST_CONJ)) return false;
+        if (s->nd_o > 1) return false;
+        if (s->nd_o == 1 && (s->o_stride[0] != TC_L || s->o_shift[0] != 0 || s->o_bound[0] != s->o_shape[0]))
+            return false;
+    }
+    return true;
+}
+
+size_t tc_smem_bytes() { return sizeof(TcSmem) + 128; }
+
+cudaError_t tc_launch(const PassParams& p, int64_t /*nblocks*/, cudaStream_t st) {
+    static int grid = 0;
+    const size_t smem = tc_smem_bytes();
+    if (grid == 0) {
+        cudaError_t e = cudaFuncSetAttribute(k_tc1024, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int per = 0, nsm = 0, dev = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tc1024, TC_NT, smem);
+        if (e != cudaSuccess) return e;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        // 32 tensor-memory columns a CTA: at most 16 CTAs of an SM can hold them
+        grid = std::max(1, std::min(per, 16)) * nsm;
+    }
+    const int64_t ntiles = (p.nlines + TC_LINES - 1) / TC_LINES;
+    if (ntiles <= 0) return cudaSuccess;
+    const int g = (int)std::min<int64_t>(grid, ntiles);
+    k_tc1024<<<g, TC_NT, smem, st>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace rk
