@@ -548,6 +548,87 @@ def run_serve(args, rank: int, world: int, local_rank: int) -> int:
     return 0
 
 
+# --- precision mode ---------------------------------------------------------------
+
+
+def run_precision(args, rank: int, world: int, local_rank: int) -> int:
+    """16384 x 1024 complex64 along the last axis, plain FP32 against the tensor-core
+    split-precision mode, on N(0,1) data and on a 60 dB variant (components +-10^U(-3,0))."""
+    import numpy
+    import torch
+
+    from reikna_b200 import _native as N
+    from reikna_b200.fft import FFT
+
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    shape = (16384, 1024)
+    nbytes = shape[0] * shape[1] * 8
+    b_alg = 2 * nbytes  # P_min = 1
+    peak, peak_kind = peaks()
+    out = {}
+    for label, seed in (("normal", 7), ("sixty_db", 8)):
+        rng = numpy.random.default_rng(seed)
+        if label == "normal":
+            x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(numpy.complex64)
+        else:
+            mag = 10 ** rng.uniform(-3, 0, (2,) + shape)
+            sgn = rng.choice([-1.0, 1.0], (2,) + shape)
+            x = (sgn[0] * mag[0] + 1j * sgn[1] * mag[1]).astype(numpy.complex64)
+        ref = numpy.fft.fft(x.astype(numpy.complex128), axis=1)
+        xs = [torch.from_numpy(x).to(dev), torch.from_numpy(x).to(dev)]
+        ys = [torch.empty_like(xs[0]) for _ in range(2)]
+        res = {}
+        for mode, flags in (("fp32", 0), ("split_tc", N.FLAG_SPLIT_TC)):
+            comp = FFT(xs[0], axes=(1,)).compile(dev, flags=flags)
+            plan = comp._runner.plan
+            for k in range(max(3, args.warmup)):
+                comp(None, ys[k % 2], xs[k % 2])
+            torch.cuda.synchronize(dev)
+            steps = max(1, min(args.steps, 500))
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record()
+            for k in range(steps):
+                comp(None, ys[k % 2], xs[k % 2])
+            s1.record()
+            torch.cuda.synchronize(dev)
+            ms = s0.elapsed_time(s1) / steps
+            comp(None, ys[0], xs[0])
+            y = ys[0].cpu().numpy()
+            err = float(numpy.linalg.norm((y - ref).ravel()) / numpy.linalg.norm(ref.ravel()))
+            res[mode] = {
+                "gbs": b_alg / (ms / 1e3) / 1e9,
+                "hbm_frac": b_alg / (ms / 1e3) / 1e9 / peak,
+                "us_per_step": ms * 1e3,
+                "rel_l2_vs_fp64": err,
+                "tensor_core_passes": plan.tc_passes,
+                "kernel": plan.describe()["passes"][0]["note"],
+            }
+        out[label] = res
+    line = {
+        "metric": METRIC,
+        "value": out["normal"]["split_tc"]["gbs"],
+        "unit": "GB/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": out["normal"]["split_tc"]["us_per_step"] / 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f16x2-split/f32-acc",
+        "data": "synthetic",
+        "config": {"workload": "precision_16384x1024_complex64", "shape": list(shape), "axes": [1],
+                   "bytes_per_step_algorithmic": b_alg, "l2": "inputs larger than L2, two buffer sets alternate",
+                   "peak_gbs": peak, "peak_kind": peak_kind},
+        "results": out,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -555,8 +636,9 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["own", "reference"], default="own")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["fft3d", "serve"], default="fft3d",
-                    help="fft3d: the headline 256^3 transform; serve: the request stream")
+    ap.add_argument("--workload", choices=["fft3d", "serve", "precision"], default="fft3d",
+                    help="fft3d: the headline 256^3 transform; serve: the request stream; "
+                    "precision: FP32 against the tensor-core split mode on 16384 x 1024")
     ap.add_argument("--requests", type=int, default=1000, help="serve: requests in the stream")
     ap.add_argument("--streams", type=int, default=4, help="serve: compute streams of the server")
     ap.add_argument("--load", type=float, default=0.7, help="serve: Poisson rate / served burst rate")
@@ -572,6 +654,8 @@ def main(argv=None) -> int:
         return run_reference(args, rank, world)
     if args.workload == "serve":
         return run_serve(args, rank, world, local_rank)
+    if args.workload == "precision":
+        return run_precision(args, rank, world, local_rank)
     return run_own(args, rank, world, local_rank)
 
 

@@ -38,18 +38,25 @@ namespace {
 constexpr int TC_NT = 128;     // threads = rows of one matrix product
 constexpr int TC_L = 1024;
 constexpr int TC_LINES = 2;    // lines per tile (2 x 64 vectors of 16 per stage)
-constexpr int TC_XS = 68;      // padded row, in complex elements, of the exchange buffer
 
 struct __align__(128) TcSmem {
     __half a_hi[TC_NT * 32];   // 8 KB each, canonical K-major layout
     __half a_lo[TC_NT * 32];
     __half b_hi[32 * 32];
     __half b_lo[32 * 32];
+    float2 in[TC_LINES * TC_L];  // next tile's input, fetched by a bulk copy
     float2 tw[TC_L];           // W_1024^m
-    float2 x[TC_LINES * 16 * TC_XS];
-    uint64_t bar;
+    uint64_t bar;              // matrix products done
+    uint64_t inbar;            // input tile landed
     uint32_t tmem;
 };
+
+// Between the two stages the 2 x 16 x 64 intermediate X1[line][k1][n2] is exchanged
+// through the operand tiles (a_hi and a_lo, 16 KB together), which are free once the
+// first stage's products are done; column n2 of row (line, k1) sits at n2 ^ 4 (k1 & 7)
+// so that both the stage-1 writes and the stage-2 reads spread over the banks.
+__device__ __forceinline__ float2* xbuf(TcSmem& S) { return reinterpret_cast<float2*>(S.a_hi); }
+__device__ __forceinline__ int x_idx(int row, int col) { return row * 64 + (col ^ ((row & 7) << 2)); }
 
 // element (row r, column k) of a 32-column operand in the no-swizzle K-major layout:
 // 8 x 8 core matrices of 128 contiguous bytes, K-adjacent ones 128 bytes apart (LBO),
@@ -104,17 +111,22 @@ __device__ __forceinline__ int tc_put_row(TcSmem& S, int row, const float2* u) {
     float m = 0.f;
 #pragma unroll
     for (int j = 0; j < 16; ++j) m = fmaxf(m, fmaxf(fabsf(u[j].x), fabsf(u[j].y)));
-    const int e = m > 0.f ? 14 - ilogbf(m) : 0;
+    // exponent field of m (zero and subnormals read as -127); the clamp keeps both
+    // 2^e and 2^-e normal floats, so scaling by them is exact
+    const int e = m > 0.f ? min(125, max(-125, 14 - ((__float_as_int(m) >> 23) - 127))) : 0;
+    const float f = __int_as_float((127 + e) << 23);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-        // column chunk c holds k = 8c .. 8c+7: real parts (c < 2) or imaginary parts
-        __align__(16) __half hi[8], lo[8];
+        // column chunk c holds k = 8c .. 8c+7: real parts (c < 2) or imaginary parts;
+        // pairs convert with one f16x2 rounding each
+        __align__(16) __half2 hi[4], lo[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int j = (c & 1) * 8 + i;
-            const float v = ldexpf(c < 2 ? u[j].x : u[j].y, e);
-            hi[i] = __float2half_rn(v);
-            lo[i] = __float2half_rn(v - __half2float(hi[i]));
+        for (int i = 0; i < 4; ++i) {
+            const int j = (c & 1) * 8 + 2 * i;
+            const float2 v = c < 2 ? make_float2(u[j].x * f, u[j + 1].x * f) : make_float2(u[j].y * f, u[j + 1].y * f);
+            hi[i] = __float22half2_rn(v);
+            const float2 h = __half22float2(hi[i]);
+            lo[i] = __float22half2_rn(make_float2(v.x - h.x, v.y - h.y));
         }
         *reinterpret_cast<uint4*>(&S.a_hi[op_idx(row, 8 * c)]) = *reinterpret_cast<const uint4*>(hi);
         *reinterpret_cast<uint4*>(&S.a_lo[op_idx(row, 8 * c)]) = *reinterpret_cast<const uint4*>(lo);
@@ -125,9 +137,14 @@ __device__ __forceinline__ int tc_put_row(TcSmem& S, int row, const float2* u) {
 // one radix-16 stage of the 128 rows: split products into tensor memory, then this
 // thread's row back, scaled by 2^-e; false if the wait ran out
 __device__ __forceinline__ bool tc_stage(TcSmem& S, uint32_t tmem, uint32_t& phase, int e, float2* y,
-                                         int32_t* status) {
+                                         int32_t* status, const float2* next = nullptr, uint32_t next_bytes = 0) {
     fence_proxy_async_smem();
     __syncthreads();
+    if (threadIdx.x == 0 && next_bytes) {
+        // every thread has read the input buffer: fetch the next tile into it
+        mbar_arrive_expect_tx(&S.inbar, next_bytes);
+        bulk_g2s(S.in, next, next_bytes, &S.inbar);
+    }
     if (threadIdx.x == 0) {
         tc_fence_after();
 #pragma unroll
@@ -150,8 +167,9 @@ __device__ __forceinline__ bool tc_stage(TcSmem& S, uint32_t tmem, uint32_t& pha
     float v[32];
     const uint32_t warp = threadIdx.x >> 5;
     tc_ld_row(tmem + ((warp * 32) << 16), v);
+    const float g = __int_as_float((127 - e) << 23);
 #pragma unroll
-    for (int q = 0; q < 16; ++q) y[q] = make_float2(ldexpf(v[q], -e), ldexpf(v[16 + q], -e));
+    for (int q = 0; q < 16; ++q) y[q] = make_float2(v[q] * g, v[16 + q] * g);
     return true;
 }
 
@@ -182,6 +200,7 @@ __global__ void __launch_bounds__(TC_NT) k_tc1024(const __grid_constant__ PassPa
     }
     if (t == 0) {
         mbar_init(&S.bar, 1);
+        mbar_init(&S.inbar, 1);
         fence_mbar_init();
     }
     if (warp == 0) {
@@ -204,7 +223,21 @@ __global__ void __launch_bounds__(TC_NT) k_tc1024(const __grid_constant__ PassPa
     const float2* src = reinterpret_cast<const float2*>(ld.ptr) + ld.offset;
     float2* dst = reinterpret_cast<float2*>(st.ptr) + st.offset;
     const int64_t ntiles = (p.nlines + TC_LINES - 1) / TC_LINES;
-    uint32_t phase = 0;
+    uint32_t phase = 0, iphase = 0;
+    // input tiles come by bulk copy when the array sits on the 16-byte grid the copy
+    // needs, else by plain loads
+    const bool bulk = (reinterpret_cast<uintptr_t>(src) & 15) == 0;
+    auto tile_bytes = [&](int64_t tile) -> uint32_t {
+        if (tile >= ntiles) return 0;
+        const int64_t lines = std::min<int64_t>(TC_LINES, p.nlines - tile * TC_LINES);
+        return (uint32_t)(lines * TC_L * sizeof(float2));
+    };
+    bool pending = false;  // thread 0: a bulk copy is in flight
+    if (bulk && t == 0 && blockIdx.x < ntiles) {
+        pending = true;
+        mbar_arrive_expect_tx(&S.inbar, tile_bytes(blockIdx.x));
+        bulk_g2s(S.in, src + (int64_t)blockIdx.x * TC_LINES * TC_L, tile_bytes(blockIdx.x), &S.inbar);
+    }
 
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         // ---- stage 1: radix 16 over n1 of n = 64 n1 + n2; row t = (line, n2) ----
@@ -213,19 +246,33 @@ __global__ void __launch_bounds__(TC_NT) k_tc1024(const __grid_constant__ PassPa
             const int64_t line = tile * TC_LINES + ll;
             const bool ok = line < p.nlines;
             float2 u[16];
+            if (bulk) {
+                bool landed = mbar_wait(&S.inbar, iphase, p.status);
+                if (landed) {
+                    iphase ^= 1;
+                    pending = false;
+                }
+                if (!__syncthreads_and(landed)) break;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) u[j] = ok ? S.in[ll * TC_L + 64 * j + n2] : make_float2(0.f, 0.f);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) u[j] = ok ? src[line * TC_L + 64 * j + n2] : make_float2(0.f, 0.f);
+            }
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
-                float2 v = ok ? src[line * TC_L + 64 * j + n2] : make_float2(0.f, 0.f);
-                if (ld_scale) v = cmulf(v, lsc);
-                if (ld_conj) v.y = -v.y;
-                u[j] = v;
+                if (ld_scale) u[j] = cmulf(u[j], lsc);
+                if (ld_conj) u[j].y = -u[j].y;
             }
             const int e = tc_put_row(S, t, u);
             float2 y[16];
-            if (!tc_stage(S, tmem, phase, e, y, p.status)) break;
+            const int64_t nxt = tile + gridDim.x;
+            if (t == 0) pending = bulk && tile_bytes(nxt) > 0;
+            if (!tc_stage(S, tmem, phase, e, y, p.status, src + nxt * TC_LINES * TC_L, bulk ? tile_bytes(nxt) : 0))
+                break;
             // twiddle W_1024^(n2 k1), then X1[line][k1][n2] to the exchange buffer
 #pragma unroll
-            for (int k1 = 0; k1 < 16; ++k1) S.x[(ll * 16 + k1) * TC_XS + n2] = cmulf(y[k1], S.tw[(n2 * k1) & (TC_L - 1)]);
+            for (int k1 = 0; k1 < 16; ++k1) xbuf(S)[x_idx(ll * 16 + k1, n2)] = cmulf(y[k1], S.tw[(n2 * k1) & (TC_L - 1)]);
         }
         tc_fence_before();
         __syncthreads();
@@ -234,7 +281,8 @@ __global__ void __launch_bounds__(TC_NT) k_tc1024(const __grid_constant__ PassPa
             const int ll = t >> 6, k1 = (t >> 2) & 15, m2 = t & 3;
             float2 u[16];
 #pragma unroll
-            for (int m1 = 0; m1 < 16; ++m1) u[m1] = S.x[(ll * 16 + k1) * TC_XS + 4 * m1 + m2];
+            for (int m1 = 0; m1 < 16; ++m1) u[m1] = xbuf(S)[x_idx(ll * 16 + k1, 4 * m1 + m2)];
+            __syncthreads();  // the exchange buffer becomes the operand tiles again
             const int e = tc_put_row(S, t, u);
             float2 y[16];
             if (!tc_stage(S, tmem, phase, e, y, p.status)) break;
@@ -272,6 +320,8 @@ __global__ void __launch_bounds__(TC_NT) k_tc1024(const __grid_constant__ PassPa
         tc_fence_before();
         __syncthreads();
     }
+    // a copy still in flight after a timed-out wait lands before the CTA leaves
+    if (pending) mbar_wait(&S.inbar, iphase, p.status);
     // all tensor-memory reads are done (or abandoned after a timed-out wait)
     tc_fence_before();
     __syncthreads();
@@ -304,13 +354,18 @@ cudaError_t tc_launch(const PassParams& p, int64_t /*nblocks*/, cudaStream_t st)
     if (grid == 0) {
         cudaError_t e = cudaFuncSetAttribute(k_tc1024, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        int per = 0, nsm = 0, dev = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tc1024, TC_NT, smem);
+        int nsm = 0, dev = 0, smem_sm = 0;
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, k_tc1024);
         if (e != cudaSuccess) return e;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        // 32 tensor-memory columns a CTA: at most 16 CTAs of an SM can hold them
-        grid = std::max(1, std::min(per, 16)) * nsm;
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        // resident CTAs by shared memory (1 KB reserved a CTA) and registers; 32
+        // tensor-memory columns a CTA: at most 16 CTAs of an SM can hold them
+        const int by_smem = smem_sm / (int)(smem + 1024);
+        const int by_regs = 65536 / std::max(1, fa.numRegs * TC_NT);
+        grid = std::max(1, std::min({by_smem, by_regs, 16})) * nsm;
     }
     const int64_t ntiles = (p.nlines + TC_LINES - 1) / TC_LINES;
     if (ntiles <= 0) return cudaSuccess;

@@ -104,3 +104,24 @@ def test_split_tc_device_status_clean():
     x = normal_array(numpy.random.default_rng(14), (256, 1024), numpy.complex64)
     _run(x, N.FLAG_SPLIT_TC)
     assert N.device_status(clear=True) == 0
+
+
+def test_split_tc_view_off_the_16_byte_grid():
+    # a view starting 8 bytes into its allocation takes plain loads instead of bulk copies
+    import torch
+
+    from reikna_b200 import _native as N
+    from reikna_b200.fft import FFT
+
+    rng = numpy.random.default_rng(15)
+    x = normal_array(rng, (5, 1024), numpy.complex64)
+    base = torch.zeros(5 * 1024 + 1, dtype=torch.complex64, device="cuda")
+    view = base[1:].view(5, 1024)
+    view.copy_(torch.from_numpy(x))
+    out = torch.empty_like(view)
+    c = FFT(view, axes=(1,)).compile(flags=N.FLAG_SPLIT_TC)
+    c(None, out, view)
+    torch.cuda.synchronize()
+    assert c._runner.plan.tc_passes == 1
+    ref = numpy.fft.fft(x.astype(numpy.complex128), axis=1)
+    assert rel_l2(out.cpu().numpy(), ref) < fft_bound(numpy.complex64, 1024)
