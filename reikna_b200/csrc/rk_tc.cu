@@ -45,7 +45,7 @@ struct __align__(128) TcSmem {
     __half b_hi[32 * 32];
     __half b_lo[32 * 32];
     float2 in[TC_LINES * TC_L];  // next tile's input, fetched by a bulk copy
-    float2 tw[TC_L];           // W_1024^m
+    float2 tw[TC_L];           // stage twiddles of the 1024-point plan (TwLayout order)
     uint64_t bar;              // matrix products done
     uint64_t inbar;            // input tile landed
     uint32_t tmem;
@@ -181,13 +181,17 @@ __global__ void __launch_bounds__(TC_NT) k_tc1024(const __grid_constant__ PassPa
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
     TcSmem& S = *reinterpret_cast<TcSmem*>(tc_smem_raw);
     const int t = threadIdx.x;
-    const int warp = t >> 5, lane = t & 31;
+    const int warp = t >> 5;
 
-    // tables: W_1024^m and the real 32 x 32 DFT-16 matrix B[n][k] (K-major) as hi / lo
+    // the FP64-generated stage twiddles of the pass (stage 0: W_1024^(n2 k1) at
+    // [k1 - 1][n2]; stage 1: W_64^(m2 q1) at 960 + [q1 - 1][m2]) and the real 32 x 32
+    // DFT-16 matrix B[n][k] (K-major) as hi / lo
+    static_assert(Radix<float, TC_L>::NS == 3 && Radix<float, TC_L>::R[0] == 16 && Radix<float, TC_L>::R[1] == 16 &&
+                      Radix<float, TC_L>::R[2] == 4 && TwLayout<float, TC_L>::total() == 1020,
+                  "the tensor-core pass follows the 16 x 16 x 4 plan of 1024-point lines");
+    const float2* stw = reinterpret_cast<const float2*>(p.tw);
     for (int e = t; e < TC_L; e += TC_NT) {
-        double s, c;
-        sincospi(-2.0 * e / TC_L, &s, &c);
-        S.tw[e] = make_float2((float)c, (float)s);
+        if (e < 1020) S.tw[e] = stw[e];
         const int n = e >> 5, k = e & 31;
         const int m = ((k & 15) * (n & 15)) & 15;
         double sv, cv;
@@ -272,7 +276,8 @@ __global__ void __launch_bounds__(TC_NT) k_tc1024(const __grid_constant__ PassPa
                 break;
             // twiddle W_1024^(n2 k1), then X1[line][k1][n2] to the exchange buffer
 #pragma unroll
-            for (int k1 = 0; k1 < 16; ++k1) xbuf(S)[x_idx(ll * 16 + k1, n2)] = cmulf(y[k1], S.tw[(n2 * k1) & (TC_L - 1)]);
+            for (int k1 = 0; k1 < 16; ++k1)
+                xbuf(S)[x_idx(ll * 16 + k1, n2)] = k1 ? cmulf(y[k1], S.tw[(k1 - 1) * 64 + n2]) : y[0];
         }
         tc_fence_before();
         __syncthreads();
@@ -286,35 +291,40 @@ __global__ void __launch_bounds__(TC_NT) k_tc1024(const __grid_constant__ PassPa
             const int e = tc_put_row(S, t, u);
             float2 y[16];
             if (!tc_stage(S, tmem, phase, e, y, p.status)) break;
-            // twiddle W_64^(m2 q1) = W_1024^(16 m2 q1), then radix 4 over m2 (lanes
-            // 4c .. 4c + 3 hold m2 = 0 .. 3 of the same (line, k1)):
-            //   Z[q1 + 16 q2] = sum_m2 V_m2[q1] (-i)^(m2 q2), this lane computes q2 = m2
+            // twiddle W_64^(m2 q1), then radix 4 over m2 through the (now free)
+            // operand tiles: row (line, k1) holds V_m2[q1] at column 4 q1 + m2; this
+            // thread then takes q1 = 4 m2 + i (i < 4) for all m2' and computes
+            //   Z[q1 + 16 q2] = sum_m2' V_m2'[q1] (-i)^(m2' q2),  q2 = 0 .. 3
+            const int row = ll * 16 + k1;
+#pragma unroll
+            for (int q1 = 0; q1 < 16; ++q1)
+                xbuf(S)[x_idx(row, 4 * q1 + m2)] = q1 ? cmulf(y[q1], S.tw[960 + (q1 - 1) * 4 + m2]) : y[0];
+            __syncthreads();
             const int64_t line = tile * TC_LINES + ll;
             const bool ok = line < p.nlines;
-            const int base = lane & ~3;
 #pragma unroll
-            for (int q1 = 0; q1 < 16; ++q1) {
-                const float2 w = cmulf(y[q1], S.tw[(16 * m2 * q1) & (TC_L - 1)]);
+            for (int i = 0; i < 4; ++i) {
+                const int q1 = 4 * m2 + i;
                 float2 v[4];
 #pragma unroll
-                for (int mm = 0; mm < 4; ++mm) {
-                    v[mm].x = __shfl_sync(0xffffffffu, w.x, base + mm);
-                    v[mm].y = __shfl_sync(0xffffffffu, w.y, base + mm);
-                }
-                // (-i)^(mm m2): powers of -i rotate (x, y) -> (y, -x)
-                float2 z = v[0];
+                for (int mm = 0; mm < 4; ++mm) v[mm] = xbuf(S)[x_idx(row, 4 * q1 + mm)];
+                // radix 4 with W_4 = -i
+                const float2 a = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
+                const float2 b = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+                const float2 c = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
+                const float2 d = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+                float2 z[4];
+                z[0] = make_float2(a.x + c.x, a.y + c.y);
+                z[1] = make_float2(b.x + d.y, b.y - d.x);  // b - i d
+                z[2] = make_float2(a.x - c.x, a.y - c.y);
+                z[3] = make_float2(b.x - d.y, b.y + d.x);  // b + i d
 #pragma unroll
-                for (int mm = 1; mm < 4; ++mm) {
-                    const int r = (mm * m2) & 3;
-                    const float2 a = v[mm];
-                    const float2 b = r == 0 ? a : r == 1 ? make_float2(a.y, -a.x) : r == 2 ? make_float2(-a.x, -a.y)
-                                                                                   : make_float2(-a.y, a.x);
-                    z.x += b.x;
-                    z.y += b.y;
+                for (int q2 = 0; q2 < 4; ++q2) {
+                    float2 o = z[q2];
+                    if (st_conj) o.y = -o.y;
+                    if (st_scale) o = cmulf(o, ssc);
+                    if (ok) dst[line * TC_L + k1 + 16 * q1 + 256 * q2] = o;
                 }
-                if (st_conj) z.y = -z.y;
-                if (st_scale) z = cmulf(z, ssc);
-                if (ok) dst[line * TC_L + k1 + 16 * q1 + 256 * m2] = z;
             }
         }
         tc_fence_before();
