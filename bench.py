@@ -548,6 +548,104 @@ def run_serve(args, rank: int, world: int, local_rank: int) -> int:
     return 0
 
 
+# --- batched launch -----------------------------------------------------------------
+
+
+def run_batch(args, rank: int, world: int, local_rank: int) -> int:
+    """Mixed-size batch: 1000 x 3001 (axis 1, Bluestein), 1000 x 1000 (both axes) and a
+    1000 x 1000 float32 real-to-complex transform cropped to 1000 x 501, run as plain
+    per-call execution and as one batch in each mode (calls, CUDA graph, persistent
+    launch, autotuned)."""
+    import numpy
+    import torch
+
+    from reikna_b200 import transformations as tr
+    from reikna_b200.batch import BatchedFFT
+    from reikna_b200.fft import FFT
+
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    rng4, rng5, rng6 = (numpy.random.default_rng(s) for s in (4, 5, 6))
+    xa = (rng4.standard_normal((1000, 3001)) + 1j * rng4.standard_normal((1000, 3001))).astype(numpy.complex64)
+    xb = (rng5.standard_normal((1000, 1000)) + 1j * rng5.standard_normal((1000, 1000))).astype(numpy.complex64)
+    xc = rng6.uniform(-1, 1, (1000, 1000)).astype(numpy.float32)
+    ta, tb, tc = (torch.from_numpy(x).to(dev) for x in (xa, xb, xc))
+    fa = FFT(ta, axes=(1,))
+    fb = FFT(tb, axes=(0, 1))
+    r2c = tr.real_to_complex(tc)
+    fc = FFT(r2c.parameter.output)
+    fc.parameter.input.connect(r2c, r2c.parameter.output, real_input=r2c.parameter.input)
+    crop = tr.crop_frequencies(fc.parameter.output)
+    fc.parameter.output.connect(crop, crop.parameter.input, half=crop.parameter.output)
+    comps = [fa, fb, fc]
+    outs = [torch.empty_like(ta), torch.empty_like(tb), torch.empty((1000, 501), dtype=torch.complex64, device=dev)]
+    args_list = [(o, i) for o, i in zip(outs, (ta, tb, tc))]
+    # B_alg per member: P_min (input + output bytes); M = 8192 (P 1), 2048^2 (P 2), 2048^2 (P 2)
+    b_alg = 1 * (2 * 24_008_000) + 2 * (2 * 8_000_000) + 2 * (4_000_000 + 4_008_000)
+    refs = [
+        numpy.fft.fft(xa.astype(numpy.complex128), axis=1),
+        numpy.fft.fft2(xb.astype(numpy.complex128)),
+        numpy.fft.rfft2(xc.astype(numpy.float64)),
+    ]
+
+    def timed(fn, reps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize(dev)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(reps):
+            fn()
+        s1.record()
+        torch.cuda.synchronize(dev)
+        return s0.elapsed_time(s1) / reps
+
+    reps = max(1, min(args.steps, 200))
+    singles = [c.compile(dev) for c in comps]
+
+    def plain():
+        for cc, (o, i) in zip(singles, args_list):
+            cc(None, o, i)
+
+    res = {"plain_per_call": {"us": timed(plain, reps) * 1e3}}
+    for mode in ("calls", "graph", "persistent", "auto"):
+        bat = BatchedFFT(comps, device=dev, mode=mode)
+        ms = timed(lambda: bat(None, args_list), reps)
+        errs = [float(numpy.linalg.norm((o.cpu().numpy() - r).ravel()) / numpy.linalg.norm(r.ravel())) for o, r in zip(outs, refs)]
+        entry = {"us": ms * 1e3, "rel_l2_vs_fp64": errs, "chosen": list(bat.chosen)}
+        if mode == "persistent":
+            entry["launch"] = bat._variant.batch.info()
+        if mode == "auto":
+            entry["tried"] = bat.tuning.get("tried") if bat.tuning else None
+        res[mode] = entry
+        bat.close()
+    for k, v in res.items():
+        v["gbs"] = b_alg / (v["us"] / 1e6) / 1e9
+    best = min((k for k in res if k != "plain_per_call"), key=lambda k: res[k]["us"])
+    line = {
+        "metric": METRIC,
+        "value": res["auto"]["gbs"],
+        "unit": "GB/s",
+        "n_gpus": 1,
+        "steps": reps,
+        "warmup": args.warmup,
+        "ms_per_step": res["auto"]["us"] / 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "batch_1000x3001_1000x1000_r2c1000x1000", "bytes_per_step_algorithmic": b_alg,
+                   "fastest_mode": best},
+        "modes": res,
+        "speedup_vs_plain": res["plain_per_call"]["us"] / res["auto"]["us"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # --- precision mode ---------------------------------------------------------------
 
 
@@ -636,9 +734,10 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["own", "reference"], default="own")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["fft3d", "serve", "precision"], default="fft3d",
+    ap.add_argument("--workload", choices=["fft3d", "serve", "precision", "batch"], default="fft3d",
                     help="fft3d: the headline 256^3 transform; serve: the request stream; "
-                    "precision: FP32 against the tensor-core split mode on 16384 x 1024")
+                    "precision: FP32 against the tensor-core split mode on 16384 x 1024; "
+                    "batch: the mixed-size batch in every batching mode")
     ap.add_argument("--requests", type=int, default=1000, help="serve: requests in the stream")
     ap.add_argument("--streams", type=int, default=4, help="serve: compute streams of the server")
     ap.add_argument("--load", type=float, default=0.7, help="serve: Poisson rate / served burst rate")
@@ -656,6 +755,8 @@ def main(argv=None) -> int:
         return run_serve(args, rank, world, local_rank)
     if args.workload == "precision":
         return run_precision(args, rank, world, local_rank)
+    if args.workload == "batch":
+        return run_batch(args, rank, world, local_rank)
     return run_own(args, rank, world, local_rank)
 
 
