@@ -73,6 +73,8 @@ extern "C" {
                                 contiguous complex64 line passes; others run as usual) */
 #define RK_FLAG_PLANE_WIDE 8 /* plane pass on twice as many CTAs per cluster (tuning) */
 #define RK_FLAG_NO_TMA 16    /* never use the persistent TMA-fed line passes */
+#define RK_FLAG_PAIR 32      /* two innermost power-of-two axes: row and column passes in one
+                                plane-ordered launch instead of the clustered plane pass */
 
 /*
  * One side (input or output) of the FFT as the user sees it after the

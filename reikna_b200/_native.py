@@ -40,6 +40,7 @@ FLAG_NO_BLUE1 = 2
 FLAG_SPLIT_TC = 4
 FLAG_PLANE_WIDE = 8
 FLAG_NO_TMA = 16
+FLAG_PAIR = 32
 
 EXPORTED = (
     "rk_edge_init",

@@ -53,6 +53,13 @@ struct PlaneInfo {
 bool line_info(int dbl, int L, int mode, int var, LineInfo* out);
 bool plane_info(int dbl, int L1, int L2, int wide, PlaneInfo* out);
 
+// row + column passes of a plane in one persistent launch (rk_pair.cu)
+struct PairInfo {
+    cudaError_t (*launch)(const void* args, cudaStream_t st);
+    int (*resident)();   // CTAs resident at once on the device
+    int nl_rows, nl_cols;
+};
+
 struct PassRec {
     int kind = PK_LINE;
     int dbl = 0;
@@ -75,11 +82,22 @@ struct PassRec {
     int64_t plane_tma_blocks = 0;
     bool use_tma = false;
     bool use_tc = false;           // tensor-core split-precision kernel (RK_FLAG_SPLIT_TC)
+    bool pair_first = false;       // this pass and the next run as one pair launch
+    PairInfo pair{};
+    void* pair_tasks = nullptr;    // int32 task table
+    void* pair_counters = nullptr; // task counter + per-plane row-tile counters
+    int64_t pair_ntasks = 0, pair_planes = 0;
+    int32_t pair_a = 0, pair_b = 0;
     bool tma_reencode = false;     // tensor map over the user's input: re-encode per call
     const void* tma_ptr = nullptr; // pointer the current map was encoded for
     int tma_rows = 0;
     std::string note;
 };
+
+bool pair_info(int dbl, int LR, int LC, PairInfo* out);
+int pair_setup(PassRec& ra, PassRec& rb, const PairInfo& pi);
+cudaError_t pair_launch(const PassRec& ra, const PassParams& pa, const PassParams& pb, int32_t* status,
+                        cudaStream_t st);
 
 // tensor-core split-precision pass (rk_tc.cu): 1024-point complex64 contiguous lines
 bool tc_eligible(const PassRec& r);

@@ -222,6 +222,7 @@ struct PassSpec {
     bool inplace_safe = true;
     int64_t tw4_N = 0;
     int blue_axis = -1;     // fused Bluestein kernel spectrum owner
+    bool pair = false;      // with the next pass: one plane-ordered pair launch
     SideSpec ld, st;
     std::string note;
 };
@@ -277,8 +278,14 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
     }
 
     const int LM = lane_max(dbl), PM = pos_max(dbl);
-    // the two innermost dims, both transformed powers of two: one clustered pass
-    if (!(d.flags & RK_FLAG_NO_PLANE) && nd >= 2 && axes.size() >= 2 && axes[0] == nd - 1 && axes[1] == nd - 2 &&
+    // the two innermost dims, both transformed powers of two: one clustered pass, or
+    // (RK_FLAG_PAIR) a row pass and a column pass run as one plane-ordered launch
+    PairInfo pair_probe;
+    const bool want_pair = (d.flags & RK_FLAG_PAIR) && nd >= 2 && axes.size() >= 2 && axes[0] == nd - 1 &&
+                           axes[1] == nd - 2 && is_pow2(d.shape[nd - 1]) && is_pow2(d.shape[nd - 2]) &&
+                           pair_info(dbl, (int)d.shape[nd - 1], (int)d.shape[nd - 2], &pair_probe);
+    const size_t pair_at = P.passes.size();
+    if (!want_pair && !(d.flags & RK_FLAG_NO_PLANE) && nd >= 2 && axes.size() >= 2 && axes[0] == nd - 1 && axes[1] == nd - 2 &&
         is_pow2(d.shape[nd - 1]) && is_pow2(d.shape[nd - 2])) {
         PlaneInfo pi;
         if (plane_info(dbl, (int)d.shape[nd - 2], (int)d.shape[nd - 1], (d.flags & RK_FLAG_PLANE_WIDE) ? 1 : 0, &pi)) {
@@ -440,6 +447,16 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
                 P.passes.push_back(p4);
                 cur = out;
             }
+        }
+    }
+    if (want_pair && P.passes.size() >= pair_at + 2) {
+        PassSpec& pa = P.passes[pair_at];
+        const PassSpec& pb = P.passes[pair_at + 1];
+        if (pa.note == "single" && pb.note == "single" && pa.mode == MODE_POS && pb.mode == MODE_LANE &&
+            pa.axis == nd - 1 && pb.axis == nd - 2 && pb.I == d.shape[nd - 1]) {
+            pa.pair = true;
+            pa.note = "pair-rows";
+            P.passes[pair_at + 1].note = "pair-cols";
         }
     }
     for (auto& p : P.passes) {
@@ -1000,6 +1017,17 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         }
         plan->passes.push_back(r);
     }
+    for (size_t i = 0; i + 1 < plan->passes.size(); ++i) {
+        if (!P.passes[i].pair) continue;
+        PairInfo pi;
+        if (!pair_info(dbl, plan->passes[i].L, plan->passes[i + 1].L, &pi)) continue;
+        const int rc = pair_setup(plan->passes[i], plan->passes[i + 1], pi);
+        if (rc == RK_ERR_NOMEM || rc == RK_ERR_CUDA) {
+            set_error("pair launch set-up failed");
+            return fail(rc);
+        }
+        if (rc == RK_OK) plan->device_bytes += plan->passes[i].pair_ntasks * 4 + (plan->passes[i].pair_planes + 1) * 4;
+    }
     if (plan->passes.size() == 1) {
         // a single pass rewrites only the elements its CTA (or cluster) read, unless the
         // two edges place the same logical element at different addresses
@@ -1064,6 +1092,10 @@ int rk_fft_plan_destroy(rk_fft_plan* plan) {
     for (cudaEvent_t e : plan->prof_ev) cudaEventDestroy(e);
     for (void* p : plan->temps) cudaFree(p);
     if (plan->alias_tmp) cudaFree(plan->alias_tmp);
+    for (rk::PassRec& r : plan->passes) {
+        if (r.pair_tasks) cudaFree(r.pair_tasks);
+        if (r.pair_counters) cudaFree(r.pair_counters);
+    }
     delete plan;
     return RK_OK;
 }
@@ -1235,6 +1267,21 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
         const size_t ev = 2 * ((size_t)plan->prof_used * np + i);
         if (prof) CK(cudaEventRecord(plan->prof_ev[ev], st));
         cudaError_t e;
+        if (r.pair_first && i + 1 < np) {
+            // rows and columns in one launch: the second pass records an empty interval
+            e = pair_launch(r, p, prm[i + 1], p.status, st);
+            if (e != cudaSuccess) {
+                set_error(std::string("kernel launch failed (pair): ") + cudaGetErrorString(e));
+                return RK_ERR_CUDA;
+            }
+            if (prof) {
+                CK(cudaEventRecord(plan->prof_ev[ev + 1], st));
+                CK(cudaEventRecord(plan->prof_ev[ev + 2], st));
+                CK(cudaEventRecord(plan->prof_ev[ev + 3], st));
+            }
+            ++i;
+            continue;
+        }
         if (r.kind == PK_PLANE)
             e = tma[i] ? r.pti.fn(p, r.plane_tma_blocks, st) : r.pi.fn(p, r.nblocks, st);
         else if (r.use_tc)
