@@ -170,6 +170,16 @@ RK_API int rk_fftshift_execute(void* out, const void* in, int32_t elem_bytes, in
                         int32_t inverse, void* scratch, void* stream);
 
 /*
+ * Batched transpose of a C-order array of `batch` matrices of height x width
+ * elements: out[b][w][h] = in[b][h][w]; replaces one kernel call of reikna's
+ * Transpose (reikna/algorithms/transpose.py:157-201), which realises any axis
+ * permutation as a sequence of such swaps of adjacent axis groups.  elem_bytes in
+ * {1, 2, 4, 8, 16}; pointers aligned to the element size; out may not alias in.
+ */
+RK_API int rk_transpose_execute(void* out, const void* in, int32_t elem_bytes, int64_t batch, int64_t height,
+                                int64_t width, void* stream);
+
+/*
  * Allocation-free batched 1-D complex64 FFT.  No counterpart in the reference: it
  * exists for callers that cannot allocate device memory when they need a transform
  * (code inside a memory pool or arena that owns the device, loops that must not

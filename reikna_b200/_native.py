@@ -63,6 +63,7 @@ EXPORTED = (
     "rk_batch_destroy",
     "rk_batch_info",
     "rk_fft_plan_tc_passes",
+    "rk_transpose_execute",
 )
 
 I64A = ctypes.c_int64 * MAXD
@@ -163,6 +164,7 @@ def lib() -> ctypes.CDLL:
         ]
         L.rk_fft_plan_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
         L.rk_fft_plan_tc_passes.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+        L.rk_transpose_execute.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, vp]
         L.rk_fftshift_execute.argtypes = [
             vp,
             vp,

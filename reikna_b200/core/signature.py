@@ -31,6 +31,11 @@ def _torch_dtype_map():
                 torch.float64: numpy.dtype(numpy.float64),
                 torch.int32: numpy.dtype(numpy.int32),
                 torch.int64: numpy.dtype(numpy.int64),
+                torch.int8: numpy.dtype(numpy.int8),
+                torch.uint8: numpy.dtype(numpy.uint8),
+                torch.int16: numpy.dtype(numpy.int16),
+                torch.float16: numpy.dtype(numpy.float16),
+                torch.bool: numpy.dtype(numpy.bool_),
             }
         except ImportError:  # pragma: no cover
             _TORCH_TO_NUMPY = {}

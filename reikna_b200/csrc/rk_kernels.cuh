@@ -200,7 +200,11 @@ __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, 
                 default:
                     break;
             }
-            if (s.flags & SF_WINDOW) v = cscale(v, hann<T>(u, s.win_len));
+            if (s.flags & SF_WINDOW) {
+                // the plan's FP64-generated table when present (the window ends at win_len)
+                const T w = s.win ? (u < s.win_len ? reinterpret_cast<const T*>(s.win)[u] : T(1)) : hann<T>(u, s.win_len);
+                v = cscale(v, w);
+            }
         }
     }
     const int32_t f = s.flags;
@@ -248,7 +252,11 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
     T nrm = T(0);
     if (f & SF_NORM) {
         nrm = v.x * v.x + v.y * v.y;
-        if (s.post_param != 2.0) nrm = pow(nrm, (T)(s.post_param * 0.5));
+        // |v|^order: the square root for the magnitude, no power for order 2
+        if (s.post_param == 1.0)
+            nrm = sqrt(nrm);
+        else if (s.post_param != 2.0)
+            nrm = pow(nrm, (T)(s.post_param * 0.5));
     }
     switch (s.fmt) {
         case RK_FMT_C64:

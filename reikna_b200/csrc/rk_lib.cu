@@ -171,6 +171,15 @@ __global__ void k_gen_chirp(int64_t N, int64_t M, float2* cf, double2* cd, doubl
     b[k] = make_double2(c.x, -c.y);
 }
 
+// von Hann window 0.5 (1 - cos(2 pi u / (w - 1))), u < w, in FP64, rounded once
+__global__ void k_gen_window(int32_t w, float* f, double* d) {
+    const int32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= w) return;
+    const double v = w > 1 ? 0.5 * (1.0 - cospi(2.0 * (double)u / (double)(w - 1))) : 1.0;
+    if (f) f[u] = (float)v;
+    if (d) d[u] = v;
+}
+
 __global__ void k_scale_convert(const double2* src, int64_t n, double s, float2* df, double2* dd) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -322,6 +331,12 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
                 PassSpec p;
                 p.L = (int)n;
                 p.mode = I == 1 ? MODE_POS : MODE_LANE;
+                // a last pass whose output lines are adjacent in memory while the
+                // axis is strided (a transposed output edge) stores lane-fastest
+                // through shared memory
+                if (I == 1 && last_axis && ax > 0 && n <= LM && d.output.strides[ax] != 1 &&
+                    d.output.strides[ax - 1] == 1 && d.shape[ax - 1] > 1)
+                    p.var = 2;
                 p.axis = ax;
                 p.O = O; p.C = 1; p.I = I;
                 p.ld.buf = cur; p.ld.ax_len = n; p.ld.cA = 0; p.ld.jB = 1;
@@ -951,6 +966,15 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         mark_fast2(pp.st, dbl, ps.kind == PK_PLANE ? ps.L1 : ps.L, ps.C);
         if (!r.ld_edge) pp.ld.ptr = bufs[ps.ld.buf];
         if (!r.st_edge) pp.st.ptr = bufs[ps.st.buf];
+        if ((pp.ld.flags & SF_WINDOW) && pp.ld.win_len > 0) {
+            void* wt = nullptr;
+            const int wrc = alloc((int64_t)pp.ld.win_len * (dbl ? 8 : 4), &wt);
+            if (wrc) return fail(wrc);
+            k_gen_window<<<(pp.ld.win_len + 255) / 256, 256>>>(pp.ld.win_len, dbl ? nullptr : (float*)wt,
+                                                               dbl ? (double*)wt : nullptr);
+            CK(cudaGetLastError());
+            pp.ld.win = wt;
+        }
         if (ps.ld.chirp_axis >= 0) {
             auto& bt = blue_tabs[ps.ld.chirp_axis];
             pp.ld.chirp = bt.first;

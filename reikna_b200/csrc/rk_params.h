@@ -49,6 +49,7 @@ struct Side {
     double post_param;
     const void* chirp;
     const void* tab;
+    const void* win;      // Hann window table (win_len entries, pass precision), or null
 };
 
 // opaque 128-byte CUtensorMap (encoded on the host with cuTensorMapEncodeTiled)

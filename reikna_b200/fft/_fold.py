@@ -178,7 +178,7 @@ def fold_input(tree, root: str, fft_shape: tuple[int, ...]) -> EdgeSpec:
 def fold_output(tree, root: str, fft_shape: tuple[int, ...]) -> EdgeSpec:
     nd = len(fft_shape)
     spec = EdgeSpec(ndim=nd, shape=list(fft_shape), shift=[0] * nd)
-    state = {"real": False}
+    state = {"real": False, "transposed": False}
 
     def leaf(name: str):
         param = tree.leaf_parameters[name]
@@ -206,6 +206,13 @@ def fold_output(tree, root: str, fft_shape: tuple[int, ...]) -> EdgeSpec:
             else:
                 spec.scale_params.append((ntr.node_from_tr[op["param"]], op["div"]))
             return walk(ntr.node_from_tr["output"])
+        if k == "transpose":
+            if nd != 2:
+                raise NotImplementedError("transpose_2d expects a 2-D FFT array")
+            state["transposed"] = not state["transposed"]
+            return walk(ntr.node_from_tr["output"])
+        if state["transposed"] and k in ("shift", "crop"):
+            raise NotImplementedError(f"transformation '{k}' after transpose_2d")
         if k == "shift":
             for a in op["axes"]:
                 n = fft_shape[a]
@@ -241,10 +248,16 @@ def fold_output(tree, root: str, fft_shape: tuple[int, ...]) -> EdgeSpec:
         raise ValueError("output array rank differs from the FFT array rank")
     spec.strides = _elem_strides(meta)
     spec.shape = list(meta.shape)
+    if state["transposed"]:
+        # FFT element (i, j) lands at user element (j, i)
+        spec.strides = spec.strides[::-1]
+        spec.shape = spec.shape[::-1]
     if spec.crop is not None:
         spec.shape = [min(a, b) for a, b in zip(spec.shape, spec.crop)]
     if spec.kind == "pair":
         spec.strides2 = _elem_strides(spec.metas[1])
+        if state["transposed"]:
+            spec.strides2 = spec.strides2[::-1]
         if spec.strides2 != spec.strides:
             raise NotImplementedError("real and imaginary arrays must share strides")
     return spec

@@ -6,9 +6,11 @@ of ``nfft`` samples every ``hop`` samples (``rolling_frame``), a von Hann window
 an FFT along the frame axis, the magnitude (``norm_const(1)``) and the first
 ``nfft // 2 + 1`` bins (``crop_frequencies``).  Every step is a transformation on the
 FFT's input or output, so the whole chain runs inside the FFT's first and last pass:
-the signal is read once and the (frames, nfft // 2 + 1) float32 magnitudes are
-written once.  The reference's example ends with a separate ``Transpose``; the
-layout here is frame-major, the transpose of its bins-by-frames picture.
+the signal is read once and the float32 magnitudes are written once.  The
+reference's example ends with a separate ``Transpose`` kernel to get the
+bins-by-frames picture; here ``transposed=True`` connects ``transpose_2d`` to the
+output, which the last pass applies as it stores (lane-fastest through shared
+memory), so the (nfft // 2 + 1, frames) result costs no extra pass.
 """
 
 from __future__ import annotations
@@ -20,8 +22,9 @@ from .core import ArrayMetadata
 from .fft import FFT
 
 
-def spectrogram(signal_len: int, nfft: int = 1024, hop: int = 256) -> FFT:
-    """Computation ``(cropped: float32 (frames, nfft//2+1), flat_input: float32 (signal_len,))``."""
+def spectrogram(signal_len: int, nfft: int = 1024, hop: int = 256, transposed: bool = False) -> FFT:
+    """Computation ``(cropped: float32 (frames, nfft//2+1), flat_input: float32 (signal_len,))``,
+    or with ``transposed`` ``(picture: float32 (nfft//2+1, frames), flat_input)``."""
     if nfft < 2 or hop < 1 or signal_len < nfft:
         raise ValueError("need nfft >= 2, hop >= 1 and a signal at least one frame long")
     frame = tr.rolling_frame(ArrayMetadata((signal_len,), numpy.float32), nfft, nfft - hop, None)
@@ -40,6 +43,9 @@ def spectrogram(signal_len: int, nfft: int = 1024, hop: int = 256) -> FFT:
     fft.parameter.unwindowed_input.connect(frame, frame.parameter.output, flat_input=frame.parameter.input)
     fft.parameter.output.connect(amp, amp.parameter.input, amplitude=amp.parameter.output)
     fft.parameter.amplitude.connect(crop, crop.parameter.input, cropped=crop.parameter.output)
+    if transposed:
+        tp = tr.transpose_2d(crop.parameter.output)
+        fft.parameter.cropped.connect(tp, tp.parameter.input, picture=tp.parameter.output)
     return fft
 
 

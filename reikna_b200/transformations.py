@@ -258,6 +258,21 @@ def hanning_window(arr_t, fft_size: int) -> Transformation:
     )
 
 
+def transpose_2d(arr_t) -> Transformation:
+    """``output = input.T`` for a 2-D array (output transformation).  On an FFT output
+    it is fused into the last pass' store (no separate transpose kernel, unlike the
+    ``Transpose`` step that ends reikna's spectrogram example, demo_specgram.py:268)."""
+    meta = _meta(arr_t)
+    if len(meta.shape) != 2:
+        raise ValueError("transpose_2d expects a 2-D array")
+    out = _contig((meta.shape[1], meta.shape[0]), meta.dtype)
+    return Transformation(
+        [Parameter("output", Annotation(out, "o")), Parameter("input", Annotation(meta, "i"))],
+        connectors=["input"],
+        op={"kind": "transpose"},
+    )
+
+
 def crop_frequencies(arr_t) -> Transformation:
     """Keeps the first cols // 2 + 1 columns of a 2-D array (output transformation)."""
     meta = _meta(arr_t)
