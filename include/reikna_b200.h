@@ -180,6 +180,24 @@ RK_API int rk_transpose_execute(void* out, const void* in, int32_t elem_bytes, i
                                 int64_t width, void* stream);
 
 /*
+ * Real-signal transforms through a half-length complex FFT, the steps the reference
+ * runs as separate kernels around its FFT (examples/demo_specialized_fft.py:156-331,
+ * demo_specialized_fft.mako:1-62).  A real array of even length N is read by the
+ * complex FFT of length half = N / 2 as interleaved (re, im) pairs.
+ *   rk_rfft_twiddles: table[k] = exp(-2 pi i k / N), k = 0 .. half (FP64, rounded).
+ *   rk_rfft_post: out[b][k], k < half + store_last, from the half-length spectrum
+ *                 z[b][0 .. half) (out may not alias z).
+ *   rk_irfft_pre: z[b][0 .. half) from the half-spectrum x[b][0 .. half], for the
+ *                 inverse half-length FFT; imaginary parts of bins 0 and half ignored.
+ * fmt: RK_FMT_C64 or RK_FMT_C128 (the complex type of z, out, x and the table).
+ */
+RK_API int rk_rfft_twiddles(void* table, int32_t fmt, int64_t half, void* stream);
+RK_API int rk_rfft_post(void* out, const void* z, const void* table, int32_t fmt, int64_t half, int64_t batch,
+                        int32_t store_last, void* stream);
+RK_API int rk_irfft_pre(void* z, const void* x, const void* table, int32_t fmt, int64_t half, int64_t batch,
+                        void* stream);
+
+/*
  * Allocation-free batched 1-D complex64 FFT.  No counterpart in the reference: it
  * exists for callers that cannot allocate device memory when they need a transform
  * (code inside a memory pool or arena that owns the device, loops that must not

@@ -64,6 +64,9 @@ EXPORTED = (
     "rk_batch_info",
     "rk_fft_plan_tc_passes",
     "rk_transpose_execute",
+    "rk_rfft_twiddles",
+    "rk_rfft_post",
+    "rk_irfft_pre",
 )
 
 I64A = ctypes.c_int64 * MAXD
@@ -165,6 +168,9 @@ def lib() -> ctypes.CDLL:
         L.rk_fft_plan_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
         L.rk_fft_plan_tc_passes.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
         L.rk_transpose_execute.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, vp]
+        L.rk_rfft_twiddles.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, vp]
+        L.rk_rfft_post.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, vp]
+        L.rk_irfft_pre.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, vp]
         L.rk_fftshift_execute.argtypes = [
             vp,
             vp,

@@ -1,0 +1,187 @@
+// Real-signal transforms through a half-length complex FFT (the reference's
+// examples/demo_specialized_fft.py:156-331 and demo_specialized_fft.mako:1-62).
+//
+// A real x of even length N, read as the complex z[n] = x[2n] + i x[2n+1] of length
+// H = N / 2, has Z = FFT_H(z) and
+//     X[k] = Z[k] A[k] + conj(Z[(H - k) mod H]) B[k],   k = 0 .. H,
+//     A[k] = (1 - i W^k) / 2,  B[k] = (1 + i W^k) / 2,  W = exp(-2 pi i / N);
+// the inverse takes Z[k] = X[k] conj(A[k]) + conj(X[H - k]) conj(B[k]) and
+// z = IFFT_H(Z).  W^k (k = 0 .. H) is tabulated once in FP64 and rounded to the
+// working precision.  Both kernels are element-wise over (batch, k): one read of
+// each input element pair and one write per output element.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "rk_internal.h"
+
+namespace rk {
+
+namespace {
+
+template <typename V> struct Real;
+template <> struct Real<float2> { using T = float; };
+template <> struct Real<double2> { using T = double; };
+
+template <typename V> __device__ __forceinline__ V mk(typename Real<V>::T x, typename Real<V>::T y) {
+    V v;
+    v.x = x;
+    v.y = y;
+    return v;
+}
+
+template <typename V> __device__ __forceinline__ V mulc(V a, V b) {
+    return mk<V>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+template <typename V> __device__ __forceinline__ V conjc(V a) { return mk<V>(a.x, -a.y); }
+
+// A[k] = (1 - i w) / 2, B[k] = (1 + i w) / 2 with w = W^k
+template <typename V> __device__ __forceinline__ void ab(V w, V& a, V& b) {
+    using T = typename Real<V>::T;
+    a = mk<V>(T(0.5) * (T(1) + w.y), T(-0.5) * w.x);
+    b = mk<V>(T(0.5) * (T(1) - w.y), T(0.5) * w.x);
+}
+
+template <typename V>
+__global__ void k_rfft_twiddles(V* w, int64_t half) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > half) return;
+    double s, c;
+    sincospi(-(double)k / (double)half, &s, &c);  // exp(-2 pi i k / N), N = 2 half
+    w[k] = mk<V>((typename Real<V>::T)c, (typename Real<V>::T)s);
+}
+
+template <typename V>
+__global__ void k_rfft_post(V* __restrict__ out, const V* __restrict__ z, const V* __restrict__ w, int64_t half,
+                            int64_t batch, int64_t out_len) {
+    const int64_t n = batch * out_len;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = e / out_len, k = e % out_len;
+        const V* zr = z + b * half;
+        const V zk = zr[k == half ? 0 : k];
+        const V zc = conjc(zr[k == 0 ? 0 : half - k]);
+        V a, bb;
+        ab(w[k], a, bb);
+        const V x = mulc(zk, a);
+        const V y = mulc(zc, bb);
+        out[b * out_len + k] = mk<V>(x.x + y.x, x.y + y.y);
+    }
+}
+
+template <typename V>
+__global__ void k_irfft_pre(V* __restrict__ z, const V* __restrict__ x, const V* __restrict__ w, int64_t half,
+                            int64_t batch) {
+    const int64_t n = batch * half;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = e / half, k = e % half;
+        const V* xr = x + b * (half + 1);
+        V xk = xr[k];
+        V xc = xr[half - k];
+        // a real signal's bins 0 and H are real: their imaginary parts are ignored,
+        // as numpy's irfft does
+        if (k == 0) {
+            xk.y = 0;
+            xc.y = 0;
+        }
+        xc = conjc(xc);
+        V a, bb;
+        ab(w[k], a, bb);
+        const V p = mulc(xk, conjc(a));
+        const V q = mulc(xc, conjc(bb));
+        z[b * half + k] = mk<V>(p.x + q.x, p.y + q.y);
+    }
+}
+
+int grid_for(int64_t n) {
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (!nsm) nsm = 148;
+    }
+    const int64_t blocks = (n + 255) / 256;
+    return (int)(blocks < (int64_t)nsm * 16 ? (blocks > 0 ? blocks : 1) : (int64_t)nsm * 16);
+}
+
+int check_fmt(int32_t fmt, const char* who) {
+    if (fmt != RK_FMT_C64 && fmt != RK_FMT_C128) {
+        set_error(std::string(who) + ": format must be RK_FMT_C64 or RK_FMT_C128");
+        return RK_ERR_INVALID;
+    }
+    return RK_OK;
+}
+
+int finish(const char* who) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string(who) + ": " + cudaGetErrorString(e));
+        return RK_ERR_CUDA;
+    }
+    return RK_OK;
+}
+
+}  // namespace
+
+}  // namespace rk
+
+using namespace rk;
+
+extern "C" int rk_rfft_twiddles(void* table, int32_t fmt, int64_t half, void* stream) {
+    if (int rc = check_fmt(fmt, "rk_rfft_twiddles")) return rc;
+    if (!table || half < 1) {
+        set_error("rk_rfft_twiddles: null table or half length < 1");
+        return RK_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned g = (unsigned)((half + 256) / 256);
+    if (fmt == RK_FMT_C64)
+        k_rfft_twiddles<float2><<<g, 256, 0, st>>>((float2*)table, half);
+    else
+        k_rfft_twiddles<double2><<<g, 256, 0, st>>>((double2*)table, half);
+    return finish("rk_rfft_twiddles");
+}
+
+extern "C" int rk_rfft_post(void* out, const void* z, const void* table, int32_t fmt, int64_t half, int64_t batch,
+                            int32_t store_last, void* stream) {
+    if (int rc = check_fmt(fmt, "rk_rfft_post")) return rc;
+    if (!out || !z || !table || half < 1 || batch < 1) {
+        set_error("rk_rfft_post: null pointer or non-positive size");
+        return RK_ERR_INVALID;
+    }
+    if (out == z) {
+        set_error("rk_rfft_post: output may not alias the half-length spectrum");
+        return RK_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t out_len = half + (store_last ? 1 : 0);
+    const int g = grid_for(batch * out_len);
+    if (fmt == RK_FMT_C64)
+        k_rfft_post<float2><<<g, 256, 0, st>>>((float2*)out, (const float2*)z, (const float2*)table, half, batch, out_len);
+    else
+        k_rfft_post<double2><<<g, 256, 0, st>>>((double2*)out, (const double2*)z, (const double2*)table, half, batch,
+                                                 out_len);
+    return finish("rk_rfft_post");
+}
+
+extern "C" int rk_irfft_pre(void* z, const void* x, const void* table, int32_t fmt, int64_t half, int64_t batch,
+                            void* stream) {
+    if (int rc = check_fmt(fmt, "rk_irfft_pre")) return rc;
+    if (!z || !x || !table || half < 1 || batch < 1) {
+        set_error("rk_irfft_pre: null pointer or non-positive size");
+        return RK_ERR_INVALID;
+    }
+    if (z == x) {
+        set_error("rk_irfft_pre: output may not alias the spectrum");
+        return RK_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int g = grid_for(batch * half);
+    if (fmt == RK_FMT_C64)
+        k_irfft_pre<float2><<<g, 256, 0, st>>>((float2*)z, (const float2*)x, (const float2*)table, half, batch);
+    else
+        k_irfft_pre<double2><<<g, 256, 0, st>>>((double2*)z, (const double2*)x, (const double2*)table, half, batch);
+    return finish("rk_irfft_pre");
+}

@@ -1,4 +1,5 @@
 from .fft import FFT
 from .fftshift import FFTShift
+from .rfft import IRFFT, RFFT
 
-__all__ = ["FFT", "FFTShift"]
+__all__ = ["FFT", "FFTShift", "RFFT", "IRFFT"]
