@@ -355,6 +355,28 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
         }
+    } else if (f & SF_FASTR) {
+        // real input of the pass precision (e.g. windowed signal frames): one line
+        // pointer, 32-bit offsets, the window from the plan's table
+        const T* lp = reinterpret_cast<const T*>(s.ptr) + la.base;
+        const T* wt = (f & SF_WINDOW) ? reinterpret_cast<const T*>(s.win) : nullptr;
+        const int st = (int)s.ax_stride;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const int a = pos(i);
+            T x = la.ok ? lp[a * st] : T(0);
+            if (wt) x *= __ldg(wt + a);
+            v[i] = cmk<V>(x, T(0));
+        }
+        if (f & SF_SCALE) {
+            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
+        }
+        if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
+        }
     } else {
 #pragma unroll
         for (int i = 0; i < N; ++i) v[i] = side_load<T>(s, la, pos(i));
@@ -416,6 +438,38 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
             for (int i = 0; i < N; ++i) {
                 const int a = a0 + pos(i) * jB;
                 if (a < bound) lp[a * st] = v[i];
+            }
+        }
+    } else if (f & SF_FASTR) {
+        // real output of the pass precision (real part or |v|^order, e.g. magnitudes),
+        // positions at or beyond the axis bound are cropped
+        if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
+        }
+        if (f & SF_SCALE) {
+            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
+        }
+        if (la.ok) {
+            T* lp = reinterpret_cast<T*>(s.ptr) + la.base;
+            const int st = (int)s.ax_stride, bound = (int)s.ax_bound;
+            const bool norm = f & SF_NORM;
+            const T order = (T)s.post_param;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int a = pos(i);
+                if (a >= bound) continue;
+                T r = v[i].x;
+                if (norm) {
+                    r = v[i].x * v[i].x + v[i].y * v[i].y;
+                    if (order == T(1))
+                        r = sqrt(r);
+                    else if (order != T(2))
+                        r = pow(r, order * T(0.5));
+                }
+                lp[a * st] = r;
             }
         }
     } else {

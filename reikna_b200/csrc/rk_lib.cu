@@ -651,6 +651,24 @@ static void mark_fast2(Side& s, int dbl, int64_t L, int64_t C) {
     s.flags |= SF_FAST2;
 }
 
+// Real sides of the pass precision with the plain index map a = j (signal frames in,
+// magnitudes or real parts out) take SF_FASTR; a windowed load needs the plan's
+// window table.
+static void mark_fastr(Side& s, int dbl, int64_t L, bool load) {
+    if (s.flags & (SF_FAST | SF_FAST2)) return;
+    const int fmt = dbl ? RK_FMT_F64 : RK_FMT_F32;
+    if (s.fmt != fmt || s.cA != 0 || s.jB != 1 || s.ax_shift != 0 || s.ax_stride < 0 || s.ax_len != L) return;
+    if ((L - 1) * std::max<int64_t>(s.ax_stride, 1) >= (int64_t(1) << 31)) return;
+    const int32_t conj = SF_PRE_CONJ | SF_POST_CONJ | SF_SCALE;
+    if (load) {
+        if (s.ax_bound != s.ax_len || (s.flags & ~(conj | SF_WINDOW))) return;
+        if ((s.flags & SF_WINDOW) && (!s.win || s.win_len < L)) return;  // the table covers every position
+    } else {
+        if (s.ax_bound > s.ax_len || (s.flags & ~(conj | SF_NORM))) return;
+    }
+    s.flags |= SF_FASTR;
+}
+
 static int validate(const rk_fft_desc* d) {
     if (!d) { set_error("null descriptor"); return RK_ERR_INVALID; }
     if (d->dtype != RK_FMT_C64 && d->dtype != RK_FMT_C128) {
@@ -974,6 +992,10 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
                                                                dbl ? (double*)wt : nullptr);
             CK(cudaGetLastError());
             pp.ld.win = wt;
+        }
+        if (ps.kind == PK_LINE) {
+            mark_fastr(pp.ld, dbl, ps.L, true);
+            mark_fastr(pp.st, dbl, ps.L, false);
         }
         if (ps.ld.chirp_axis >= 0) {
             auto& bt = blue_tabs[ps.ld.chirp_axis];

@@ -24,6 +24,7 @@ enum SideFlags : int32_t {
     SF_TW4 = 128,       // store side: multiply by W_tw4N^(c * k) (four-step twiddle)
     SF_FAST = 256,      // pass-dtype side, a = j, no axis padding, power-of-two axis
     SF_FAST2 = 512,     // pass-dtype side, a = c cA + j jB, no remap, 32-bit offsets
+    SF_FASTR = 1024,    // real side of the pass precision, a = j, no remap, 32-bit offsets
 };
 
 // Addressing of one buffer in a pass.  A line l in [0, O*C*I) decomposes as

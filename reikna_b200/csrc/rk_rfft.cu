@@ -53,48 +53,53 @@ __global__ void k_rfft_twiddles(V* w, int64_t half) {
     w[k] = mk<V>((typename Real<V>::T)c, (typename Real<V>::T)s);
 }
 
+// one CTA a row at a time (grid-stride over rows), threads across the row: no
+// per-element index division
 template <typename V>
 __global__ void k_rfft_post(V* __restrict__ out, const V* __restrict__ z, const V* __restrict__ w, int64_t half,
                             int64_t batch, int64_t out_len) {
-    const int64_t n = batch * out_len;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t b = e / out_len, k = e % out_len;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
         const V* zr = z + b * half;
-        const V zk = zr[k == half ? 0 : k];
-        const V zc = conjc(zr[k == 0 ? 0 : half - k]);
-        V a, bb;
-        ab(w[k], a, bb);
-        const V x = mulc(zk, a);
-        const V y = mulc(zc, bb);
-        out[b * out_len + k] = mk<V>(x.x + y.x, x.y + y.y);
+        V* orow = out + b * out_len;
+        for (int64_t k = threadIdx.x; k < out_len; k += blockDim.x) {
+            const V zk = zr[k == half ? 0 : k];
+            const V zc = conjc(zr[k == 0 ? 0 : half - k]);
+            V a, bb;
+            ab(__ldg(w + k), a, bb);
+            const V x = mulc(zk, a);
+            const V y = mulc(zc, bb);
+            orow[k] = mk<V>(x.x + y.x, x.y + y.y);
+        }
     }
 }
 
 template <typename V>
 __global__ void k_irfft_pre(V* __restrict__ z, const V* __restrict__ x, const V* __restrict__ w, int64_t half,
                             int64_t batch) {
-    const int64_t n = batch * half;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t b = e / half, k = e % half;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
         const V* xr = x + b * (half + 1);
-        V xk = xr[k];
-        V xc = xr[half - k];
-        // a real signal's bins 0 and H are real: their imaginary parts are ignored,
-        // as numpy's irfft does
-        if (k == 0) {
-            xk.y = 0;
-            xc.y = 0;
+        V* zr = z + b * half;
+        for (int64_t k = threadIdx.x; k < half; k += blockDim.x) {
+            V xk = xr[k];
+            V xc = xr[half - k];
+            // a real signal's bins 0 and H are real: their imaginary parts are ignored,
+            // as numpy's irfft does
+            if (k == 0) {
+                xk.y = 0;
+                xc.y = 0;
+            }
+            xc = conjc(xc);
+            V a, bb;
+            ab(__ldg(w + k), a, bb);
+            const V p = mulc(xk, conjc(a));
+            const V q = mulc(xc, conjc(bb));
+            zr[k] = mk<V>(p.x + q.x, p.y + q.y);
         }
-        xc = conjc(xc);
-        V a, bb;
-        ab(w[k], a, bb);
-        const V p = mulc(xk, conjc(a));
-        const V q = mulc(xc, conjc(bb));
-        z[b * half + k] = mk<V>(p.x + q.x, p.y + q.y);
     }
 }
 
-int grid_for(int64_t n) {
+// CTAs for a row-per-CTA kernel: the rows, at most 16 waves of one CTA per SM
+int grid_for(int64_t rows) {
     static int nsm = 0;
     if (!nsm) {
         int dev = 0;
@@ -102,8 +107,7 @@ int grid_for(int64_t n) {
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         if (!nsm) nsm = 148;
     }
-    const int64_t blocks = (n + 255) / 256;
-    return (int)(blocks < (int64_t)nsm * 16 ? (blocks > 0 ? blocks : 1) : (int64_t)nsm * 16);
+    return (int)(rows < (int64_t)nsm * 16 ? (rows > 0 ? rows : 1) : (int64_t)nsm * 16);
 }
 
 int check_fmt(int32_t fmt, const char* who) {
@@ -157,7 +161,7 @@ extern "C" int rk_rfft_post(void* out, const void* z, const void* table, int32_t
     }
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t out_len = half + (store_last ? 1 : 0);
-    const int g = grid_for(batch * out_len);
+    const int g = grid_for(batch);
     if (fmt == RK_FMT_C64)
         k_rfft_post<float2><<<g, 256, 0, st>>>((float2*)out, (const float2*)z, (const float2*)table, half, batch, out_len);
     else
@@ -178,7 +182,7 @@ extern "C" int rk_irfft_pre(void* z, const void* x, const void* table, int32_t f
         return RK_ERR_INVALID;
     }
     cudaStream_t st = (cudaStream_t)stream;
-    const int g = grid_for(batch * half);
+    const int g = grid_for(batch);
     if (fmt == RK_FMT_C64)
         k_irfft_pre<float2><<<g, 256, 0, st>>>((float2*)z, (const float2*)x, (const float2*)table, half, batch);
     else
