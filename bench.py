@@ -574,6 +574,34 @@ def run_serve(args, rank: int, world: int, local_rank: int) -> int:
     return 0
 
 
+# --- CPU oracle beside the GPU workloads ---------------------------------------------
+
+
+def oracle_seconds(shape, axes, sample_rows=None, seconds: float = 4.0):
+    """Seconds the CPU oracle (reikna's algorithm restated, all host threads) takes
+    for one complex64 transform of ``shape`` over ``axes``; with ``sample_rows`` it
+    times that many rows of the first axis (not transformed) and scales up.
+    Returns (seconds, threads, sample description)."""
+    import numpy
+
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    rows = shape[0]
+    sub = tuple(shape) if not sample_rows or 0 in axes else (min(sample_rows, rows),) + tuple(shape[1:])
+    rng = numpy.random.default_rng(3)
+    x = (rng.standard_normal(sub) + 1j * rng.standard_normal(sub)).astype(numpy.complex64)
+    plan = oracle.Plan(sub, axes)
+    times = []
+    t_end = time.perf_counter() + seconds
+    while len(times) < 2 or (time.perf_counter() < t_end and len(times) < 20):
+        t0 = time.perf_counter()
+        plan(x, threads=threads)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times[1:]) if len(times) > 2 else times[-1]
+    return t * rows / sub[0], threads, f"{list(sub)} over axes {list(axes)}" + (f", scaled to {rows} rows" if sub[0] != rows else "")
+
+
 # --- batched launch -----------------------------------------------------------------
 
 
@@ -650,6 +678,13 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> int:
     for k, v in res.items():
         v["gbs"] = b_alg / (v["us"] / 1e6) / 1e9
     best = min((k for k in res if k != "plain_per_call"), key=lambda k: res[k]["us"])
+    cpu_s, cpu_threads, samples = 0.0, 1, []
+    if not args.no_cpu_baseline:
+        # the real-input member runs on the CPU as the complex transform it reduces to
+        for shape, axes, rows in (((1000, 3001), (1,), 100), ((1000, 1000), (0, 1), None), ((1000, 1000), (0, 1), None)):
+            t, cpu_threads, desc = oracle_seconds(shape, axes, rows)
+            cpu_s += t
+            samples.append(desc)
     line = {
         "metric": METRIC,
         "value": res["auto"]["gbs"],
@@ -668,6 +703,9 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> int:
         "modes": res,
         "speedup_vs_plain": res["plain_per_call"]["us"] / res["auto"]["us"],
     }
+    if cpu_s:
+        line["cpu_baseline"] = {"value": b_alg / cpu_s / 1e9, "unit": "GB/s", "cores": cpu_threads, "kind": "port",
+                                "sample": "; ".join(samples), "ms_per_step": cpu_s * 1e3}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -731,6 +769,11 @@ def run_precision(args, rank: int, world: int, local_rank: int) -> int:
                 "kernel": plan.describe()["passes"][0]["note"],
             }
         out[label] = res
+    cpu = None
+    if not args.no_cpu_baseline:
+        t, threads, desc = oracle_seconds(shape, (1,), 1024)
+        cpu = {"value": b_alg / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc,
+               "ms_per_step": t * 1e3}
     line = {
         "metric": METRIC,
         "value": out["normal"]["split_tc"]["gbs"],
@@ -749,6 +792,8 @@ def run_precision(args, rank: int, world: int, local_rank: int) -> int:
                    "peak_gbs": peak, "peak_kind": peak_kind},
         "results": out,
     }
+    if cpu:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0
 
