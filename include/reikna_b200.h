@@ -75,6 +75,12 @@ extern "C" {
 #define RK_FLAG_NO_TMA 16    /* never use the persistent TMA-fed line passes */
 #define RK_FLAG_PAIR 32      /* two innermost power-of-two axes: row and column passes in one
                                 plane-ordered launch instead of the clustered plane pass */
+#define RK_FLAG_REAL_POST 64 /* forward transform of the last axis (length L = N/2, a power of two
+                                of at most 8192, 4096 for complex128) of a real signal read as
+                                interleaved pairs: the single pass stores the real signal's
+                                spectrum X[0 .. L) and, when the output edge is L + 1 long, X[L]
+                                (examples/demo_specialized_fft.py:175-241 as one pass);
+                                rk_fft_execute then rejects inverse = 1 */
 
 /*
  * One side (input or output) of the FFT as the user sees it after the

@@ -41,6 +41,7 @@ FLAG_SPLIT_TC = 4
 FLAG_PLANE_WIDE = 8
 FLAG_NO_TMA = 16
 FLAG_PAIR = 32
+FLAG_REAL_POST = 64
 
 EXPORTED = (
     "rk_edge_init",

@@ -601,7 +601,41 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
         __syncthreads();
         E::run(v, sm, ln, tb, tw);
     }
-    if constexpr (VAR == 2) {
+    if constexpr (VAR == 3) {
+        // real-signal spectrum from the half-length spectrum Z of this line (the line
+        // holds x[2n] + i x[2n+1]): X[k] = Z[k] A[k] + conj(Z[(L - k) mod L]) B[k],
+        // A = (1 - i W^k) / 2, B = (1 + i W^k) / 2, W = exp(-2 pi i / 2L), with W^k from
+        // the plan's FP64-generated table in st.tab; st.post_param = 1 also stores
+        // X[L] = Re Z[0] - Im Z[0] (the Nyquist bin) after the line's L positions
+        static_assert(MODE == MODE_POS, "the real-spectrum step needs whole lines");
+#pragma unroll
+        for (int z = 0; z < RT / RL; ++z)
+#pragma unroll
+            for (int m = 0; m < RL; ++m) sm[E::sidx(ln, E::out_pos(tb, z, m))] = v[z * RL + m];
+        __syncthreads();
+        const V* wk = reinterpret_cast<const V*>(p.st.tab);
+#pragma unroll
+        for (int z = 0; z < RT / RL; ++z)
+#pragma unroll
+            for (int m = 0; m < RL; ++m) {
+                const int k = E::out_pos(tb, z, m);
+                const V zk = sm[E::sidx(ln, k)];
+                const V zc = cconj(sm[E::sidx(ln, (L - k) & (L - 1))]);
+                const V w = __ldg(wk + k);
+                const V a = cmk<V>(T(0.5) * (T(1) + w.y), T(-0.5) * w.x);
+                const V bb = cmk<V>(T(0.5) * (T(1) - w.y), T(0.5) * w.x);
+                const V x = cmul(zk, a), y = cmul(zc, bb);
+                v[z * RL + m] = cmk<V>(x.x + y.x, x.y + y.y);
+            }
+        const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
+        if (tb == 0 && la.ok && p.st.post_param == 1.0) {
+            const V z0 = sm[E::sidx(ln, 0)];
+            V xl = cmk<V>(z0.x - z0.y, T(0));
+            if (p.st.flags & SF_SCALE) xl = cmul(xl, cmk<V>((T)p.st.scale_re, (T)p.st.scale_im));
+            reinterpret_cast<V*>(p.st.ptr)[la.base + (int64_t)L * p.st.ax_stride] = xl;
+        }
+        store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
+    } else if constexpr (VAR == 2) {
         static_assert(MODE == MODE_POS, "transposed store needs position mode");
 #pragma unroll
         for (int z = 0; z < RT / RL; ++z)

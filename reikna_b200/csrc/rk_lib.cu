@@ -171,6 +171,16 @@ __global__ void k_gen_chirp(int64_t N, int64_t M, float2* cf, double2* cd, doubl
     b[k] = make_double2(c.x, -c.y);
 }
 
+// W^k = exp(-2 pi i k / 2L), k = 0 .. L, for the real-spectrum store (RK_FLAG_REAL_POST)
+__global__ void k_gen_rpost(int64_t L, float2* f, double2* d) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > L) return;
+    double s, c;
+    sincospi(-(double)k / (double)L, &s, &c);
+    if (f) f[k] = make_float2((float)c, (float)s);
+    if (d) d[k] = make_double2(c, s);
+}
+
 // von Hann window 0.5 (1 - cos(2 pi u / (w - 1))), u < w, in FP64, rounded once
 __global__ void k_gen_window(int32_t w, float* f, double* d) {
     const int32_t u = blockIdx.x * blockDim.x + threadIdx.x;
@@ -261,6 +271,10 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
     axes.erase(std::remove_if(axes.begin(), axes.end(), [&](int a) { return d.shape[a] == 1; }), axes.end());
 
     const int nd = d.ndim;
+    if ((d.flags & RK_FLAG_REAL_POST) && (d.naxes != 1 || d.axes[0] != nd - 1 || d.shape[nd - 1] < 8)) {
+        set_error("RK_FLAG_REAL_POST needs a transform of the last axis only, of at least 8 points");
+        return RK_ERR_UNSUPPORTED;
+    }
     int cur = SB_IN;
     auto array_out = [&](bool inplace_ok) -> int {
         if (inplace_ok && (cur == SB_T0 || cur == SB_T1)) return cur;
@@ -337,6 +351,9 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
                 if (I == 1 && last_axis && ax > 0 && n <= LM && d.output.strides[ax] != 1 &&
                     d.output.strides[ax - 1] == 1 && d.shape[ax - 1] > 1)
                     p.var = 2;
+                // the real-signal spectrum step fused into the store (RK_FLAG_REAL_POST)
+                if ((d.flags & RK_FLAG_REAL_POST) && I == 1 && last_axis && n >= 8 && n <= (dbl ? 4096 : 8192))
+                    p.var = 3;
                 p.axis = ax;
                 p.O = O; p.C = 1; p.I = I;
                 p.ld.buf = cur; p.ld.ax_len = n; p.ld.cA = 0; p.ld.jB = 1;
@@ -462,6 +479,15 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
                 P.passes.push_back(p4);
                 cur = out;
             }
+        }
+    }
+    if (d.flags & RK_FLAG_REAL_POST) {
+        const int ax = nd - 1;
+        if (d.naxes != 1 || d.axes[0] != ax || P.passes.size() != 1 || P.passes[0].var != 3 ||
+            d.output.strides[ax] != 1 || (d.output.shape[ax] != d.shape[ax] && d.output.shape[ax] != d.shape[ax] + 1)) {
+            set_error("RK_FLAG_REAL_POST needs a one-pass forward transform of the last axis (a power of two of "
+                      "8 to 8192 points, 4096 for complex128) with a contiguous output of L or L + 1 bins");
+            return RK_ERR_UNSUPPORTED;
         }
     }
     if (want_pair && P.passes.size() >= pair_at + 2) {
@@ -997,6 +1023,20 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             mark_fastr(pp.ld, dbl, ps.L, true);
             mark_fastr(pp.st, dbl, ps.L, false);
         }
+        if (ps.var == 3) {
+            if (pp.st.fmt != (dbl ? RK_FMT_C128 : RK_FMT_C64)) {
+                set_error("RK_FLAG_REAL_POST needs a complex output of the transform's precision");
+                return fail(RK_ERR_UNSUPPORTED);
+            }
+            void* wt = nullptr;
+            const int trc = alloc((int64_t)(ps.L + 1) * (dbl ? 16 : 8), &wt);
+            if (trc) return fail(trc);
+            k_gen_rpost<<<(unsigned)((ps.L + 256) / 256), 256>>>(ps.L, dbl ? nullptr : (float2*)wt,
+                                                                 dbl ? (double2*)wt : nullptr);
+            CK(cudaGetLastError());
+            pp.st.tab = wt;
+            pp.st.post_param = desc->output.shape[ps.axis] > ps.L ? 1.0 : 0.0;
+        }
         if (ps.ld.chirp_axis >= 0) {
             auto& bt = blue_tabs[ps.ld.chirp_axis];
             pp.ld.chirp = bt.first;
@@ -1300,6 +1340,10 @@ extern "C" {
 int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
                    int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
+    if (plan && inverse && (plan->desc.flags & RK_FLAG_REAL_POST)) {
+        set_error("a plan with RK_FLAG_REAL_POST runs forward only");
+        return RK_ERR_INVALID;
+    }
     std::vector<PassParams> prm;
     std::vector<char> tma;
     prm.reserve(4);

@@ -59,6 +59,16 @@ static bool lookup(int L_, int mode, int var, LineInfo* out) {
     RK_LI(128, MODE_POS, 2)
     RK_LI(256, MODE_POS, 2)
     RK_LI(512, MODE_POS, 2)
+    RK_LI(8, MODE_POS, 3)
+    RK_LI(16, MODE_POS, 3)
+    RK_LI(32, MODE_POS, 3)
+    RK_LI(64, MODE_POS, 3)
+    RK_LI(128, MODE_POS, 3)
+    RK_LI(256, MODE_POS, 3)
+    RK_LI(512, MODE_POS, 3)
+    RK_LI(1024, MODE_POS, 3)
+    RK_LI(2048, MODE_POS, 3)
+    RK_LI(4096, MODE_POS, 3)
     return false;
 }
 

@@ -1,6 +1,10 @@
 """Half-length real transforms: ``RFFT`` and ``IRFFT`` of reikna's specialised-FFT
 example (examples/demo_specialized_fft.py:175-331), as computations.
 
+When N/2 is a power of two the half-length FFT is a single pass (up to 8192 points
+for float32 input, 4096 for float64) and the spectrum step runs inside its store
+(``RK_FLAG_REAL_POST``): one read of the signal and one write of the spectrum.
+
 ``RFFT(arr_t, dont_store_last=False)``: real (..., N) -> complex (..., N/2 + 1)
 (or N/2 without the last bin), signature ``(output:o, input:i)``, like
 ``numpy.fft.rfft`` along the last axis.  ``IRFFT(arr_t)``: complex (..., H + 1) ->
@@ -70,6 +74,23 @@ class _Half:
         return ptr
 
 
+def _fused_plan(device, meta, store_last: int):
+    """One-pass plan (RK_FLAG_REAL_POST) when the half length allows it, else None."""
+    import torch
+
+    half = meta.shape[-1] // 2
+    cdt = _complex_for(meta.dtype)
+    fmt = N.FMT_C64 if cdt == numpy.complex64 else N.FMT_C128
+    shape = tuple(meta.shape[:-1]) + (half,)
+    d = N.desc(fmt, shape, (len(shape) - 1,), N.FLAG_REAL_POST)
+    d.output = N.edge(fmt, tuple(meta.shape[:-1]) + (half + store_last,))
+    try:
+        with torch.cuda.device(device):
+            return N.Plan(d)
+    except NotImplementedError:
+        return None
+
+
 class RFFT(Computation):
     """Spectrum of real signals along the last axis through a half-length complex FFT."""
 
@@ -93,8 +114,22 @@ class RFFT(Computation):
         if not (_contiguous(ann["input"].as_array_metadata()) and _contiguous(ann["output"].as_array_metadata())):
             raise NotImplementedError("RFFT works on C-contiguous arrays")
         meta = self._meta
-        h = _Half(device, meta.shape[:-1], meta.shape[-1] // 2, _complex_for(meta.dtype))
         store_last = 0 if self._dont_store_last else 1
+        fused = _fused_plan(device, meta, store_last)
+        if fused is not None:
+            esz = numpy.dtype(_complex_for(meta.dtype)).itemsize
+
+            def fused_runner(stream: int, args):
+                out = array_pointer(args["output"], ann["output"])
+                inp = array_pointer(args["input"], ann["input"])
+                if inp % esz:
+                    raise ValueError("the real array must start on a boundary of its complex pair type")
+                fused.execute([out], [inp], inverse=0, stream=stream)
+
+            fused_runner.launches = fused.launches
+            fused_runner.plan = fused
+            return fused_runner
+        h = _Half(device, meta.shape[:-1], meta.shape[-1] // 2, _complex_for(meta.dtype))
 
         def runner(stream: int, args):
             out = array_pointer(args["output"], ann["output"])

@@ -81,3 +81,38 @@ def test_rfft_without_last_bin_and_irfft_ignores_imaginary_edges():
     IRFFT(s).compile()(None, out, s)
     torch.cuda.synchronize()
     assert numpy.allclose(out.cpu().numpy(), numpy.fft.irfft(full.astype(numpy.complex128)), atol=1e-4, rtol=1e-4)
+
+
+def test_real_post_flag_plans_one_pass():
+    from reikna_b200 import _native as N
+
+    d = N.desc(N.FMT_C64, (64, 512), (1,), N.FLAG_REAL_POST)
+    d.output = N.edge(N.FMT_C64, (64, 513))
+    plan = N.describe(d)
+    assert len(plan["passes"]) == 1 and plan["passes"][0]["var"] == 3
+    d = N.desc(N.FMT_C64, (64, 500), (1,), N.FLAG_REAL_POST)
+    with pytest.raises(NotImplementedError):
+        N.describe(d)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,dtype", [((16384, 1024), numpy.float32), ((4, 16384), numpy.float32), ((3, 8192), numpy.float64)])
+def test_fused_rfft_is_one_launch(shape, dtype):
+    import torch
+
+    from reikna_b200.fft import RFFT
+
+    rng = numpy.random.default_rng(63)
+    x = rng.uniform(-1, 1, shape).astype(dtype)
+    t = torch.from_numpy(x).cuda()
+    cdt = torch.complex64 if dtype == numpy.float32 else torch.complex128
+    for last in (False, True):
+        n = shape[-1]
+        spec = torch.empty(shape[:-1] + (n // 2 + (0 if last else 1),), dtype=cdt, device="cuda")
+        c = RFFT(t, dont_store_last=last).compile()
+        assert c.launches == 1
+        c(None, spec, t)
+        torch.cuda.synchronize()
+        ref = numpy.fft.rfft(x.astype(numpy.float64))[..., : spec.shape[-1]]
+        ctype = numpy.complex64 if dtype == numpy.float32 else numpy.complex128
+        assert rel_l2(spec.cpu().numpy(), ref) < fft_bound(ctype, n)
