@@ -291,6 +291,24 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
 // conjugation ops) use one line pointer, 32-bit strided offsets and a power-of-two
 // mask for the index remap; the value ops run once per block with hoisted flags.
 // ------------------------------------------------------------------------------
+// the side's constant scale on a thread's block; a real scale (the usual 1/N) takes
+// two multiplications an element instead of a complex product (same results)
+template <typename T, int N>
+__device__ __forceinline__ void scale_block(const Side& s, cplx<T>* v) {
+    if (s.scale_im == 0.0) {
+        const T r = (T)s.scale_re;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            v[i].x *= r;
+            v[i].y *= r;
+        }
+    } else {
+        const cplx<T> c = cmk<cplx<T>>((T)s.scale_re, (T)s.scale_im);
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
+    }
+}
+
 template <typename T, int N, class PosF>
 __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, PosF pos, cplx<T>* v) {
     using V = cplx<T>;
@@ -305,11 +323,7 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i] = cmk<V>(T(0), T(0));
         }
-        if (f & SF_SCALE) {
-            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
-        }
+        if (f & SF_SCALE) scale_block<T, N>(s, v);
         if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
@@ -326,11 +340,7 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
             const int a = a0 + pos(i) * jB;
             v[i] = (la.ok && a < bound) ? lp[a * st] : cmk<V>(T(0), T(0));
         }
-        if (f & SF_SCALE) {
-            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
-        }
+        if (f & SF_SCALE) scale_block<T, N>(s, v);
         if (f & SF_PRE_CONJ) {
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
@@ -368,11 +378,7 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
             if (wt) x *= __ldg(wt + a);
             v[i] = cmk<V>(x, T(0));
         }
-        if (f & SF_SCALE) {
-            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
-        }
+        if (f & SF_SCALE) scale_block<T, N>(s, v);
         if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
@@ -393,11 +399,7 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
         }
-        if (f & SF_SCALE) {
-            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
-        }
+        if (f & SF_SCALE) scale_block<T, N>(s, v);
         if (la.ok) {
             V* lp = reinterpret_cast<V*>(s.ptr) + la.base;
             const int st = (int)s.ax_stride, sh = s.ax_shift, mask = (int)s.ax_len - 1;
@@ -427,11 +429,7 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
         }
-        if (f & SF_SCALE) {
-            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
-        }
+        if (f & SF_SCALE) scale_block<T, N>(s, v);
         if (la.ok) {
             V* lp = reinterpret_cast<V*>(s.ptr) + la.base;
 #pragma unroll
@@ -447,11 +445,7 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
         }
-        if (f & SF_SCALE) {
-            const V c = cmk<V>((T)s.scale_re, (T)s.scale_im);
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
-        }
+        if (f & SF_SCALE) scale_block<T, N>(s, v);
         if (la.ok) {
             T* lp = reinterpret_cast<T*>(s.ptr) + la.base;
             const int st = (int)s.ax_stride, bound = (int)s.ax_bound;
