@@ -81,6 +81,20 @@ extern "C" {
                                 spectrum X[0 .. L) and, when the output edge is L + 1 long, X[L]
                                 (examples/demo_specialized_fft.py:175-241 as one pass);
                                 rk_fft_execute then rejects inverse = 1 */
+#define RK_FLAG_REAL_PRE 128 /* inverse of RK_FLAG_REAL_POST: the input edge holds the L + 1 bins
+                                X[0 .. L] of a real signal's spectrum (the imaginary parts of
+                                X[0] and X[L] are ignored, as numpy.fft.irfft does), the first
+                                load forms the half-length spectrum, and the output holds the
+                                2L real samples numpy.fft.irfft gives, as L interleaved pairs
+                                (examples/demo_specialized_fft.py:244-331 as one pass);
+                                rk_fft_execute then rejects inverse = 0 */
+#define RK_FLAG_ANTIPERIODIC 256 /* with RK_FLAG_REAL_POST or RK_FLAG_REAL_PRE: the 2L real
+                                samples are the first half x[0 .. 2L) of an antiperiodic signal
+                                (x[n + 2L] = -x[n]) of length 4L, whose spectrum is the L odd
+                                harmonics F[k] = X[2k + 1]; REAL_POST stores F (an output edge
+                                of L bins), REAL_PRE reads F and stores x
+                                (examples/demo_specialized_fft.py:379-624, APRFFT / IAPRFFT,
+                                as one pass each) */
 
 /*
  * One side (input or output) of the FFT as the user sees it after the
@@ -202,6 +216,31 @@ RK_API int rk_rfft_post(void* out, const void* z, const void* table, int32_t fmt
                         int32_t store_last, void* stream);
 RK_API int rk_irfft_pre(void* z, const void* x, const void* table, int32_t fmt, int64_t half, int64_t batch,
                         void* stream);
+
+/*
+ * Antiperiodic real signals (examples/demo_specialized_fft.py:334-624, APRFFT /
+ * IAPRFFT): the first half x[0 .. 2 half) of a signal with x[n + 2 half] = -x[n];
+ * its spectrum is the odd harmonics F[k] = X[2k + 1], k < half.  These are the
+ * element-wise steps of the multi-kernel route (half lengths the one-pass
+ * RK_FLAG_ANTIPERIODIC plans do not cover); the reference reaches the same F through
+ * an RFFT, a cumulative sum and a reduction instead.
+ *   rk_aprfft_twiddles: table[k] = exp(-i pi (2k + 1) / (2 half)), k < half, then
+ *                       table[half + m] = exp(-i pi m / half), m < half.
+ *   rk_aprfft_twiddle:  out[b][m] = in[b][m] table[half + m] (inverse: conjugated);
+ *                       in place allowed.  Forward: before FFT_half of the pairs;
+ *                       inverse: after the inverse FFT_half, giving the pairs.
+ *   rk_aprfft_post:     F[b][k] = C[k] (1 - i w_k) + conj(C[half - 1 - k]) (1 + i w_k)
+ *                       from C = FFT_half (out may not alias z).
+ *   rk_iaprfft_pre:     C[b][k] = (F[k] conj(1 - i w_k) + conj(F[half - 1 - k])
+ *                       conj(1 + i w_k)) / 4 for the inverse FFT_half (z may not alias x).
+ */
+RK_API int rk_aprfft_twiddles(void* table, int32_t fmt, int64_t half, void* stream);
+RK_API int rk_aprfft_twiddle(void* out, const void* in, const void* table, int32_t fmt, int64_t half, int64_t batch,
+                             int32_t inverse, void* stream);
+RK_API int rk_aprfft_post(void* out, const void* z, const void* table, int32_t fmt, int64_t half, int64_t batch,
+                          void* stream);
+RK_API int rk_iaprfft_pre(void* z, const void* x, const void* table, int32_t fmt, int64_t half, int64_t batch,
+                          void* stream);
 
 /*
  * Allocation-free batched 1-D complex64 FFT.  No counterpart in the reference: it

@@ -7,6 +7,8 @@
   complex128 in FP64 arithmetic), OpenMP over lines;
 * ``radix_array``, ``global_radix_info``, ``kweights``, ``kernel_chain`` -- the
   planner restatement, pinned against golden fixtures of reikna's own planner;
+* ``rfft_half``, ``irfft_half``, ``aprfft``, ``iaprfft`` -- the real and antiperiodic
+  transforms of reikna's specialised-FFT example, over the oracle FFT;
 * ``numpy_ref`` -- the FP64 numpy reference reikna's tests compare against.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use it.
@@ -181,6 +183,85 @@ def fft(x: numpy.ndarray, axes=None, inverse: bool = False, threads: int | None 
 
 def kernel_chain(shape, axes=None, local_limit: int = 1024) -> list[dict]:
     return Plan(shape, axes, local_limit).chain()
+
+
+def _complex_of(x: numpy.ndarray):
+    return numpy.complex64 if x.dtype in (numpy.float32, numpy.complex64) else numpy.complex128
+
+
+def rfft_half(x: numpy.ndarray, threads: int | None = None) -> numpy.ndarray:
+    """Spectrum of real signals along the last axis through the half-length complex FFT
+    (examples/demo_specialized_fft.py:58-79; the RFFT computation :175-241 and the
+    ``prepare_rfft_output`` kernel of demo_specialized_fft.mako:1-33).  The half-length
+    FFT is the oracle's reikna-semantics FFT in the input's precision; the A/B step
+    runs in FP64."""
+    x = numpy.asarray(x)
+    n = x.shape[-1]
+    h = n // 2
+    z = (x[..., 0::2] + 1j * x[..., 1::2]).astype(_complex_of(x))
+    zf = fft(z, axes=(z.ndim - 1,), threads=threads).astype(numpy.complex128)
+    w = numpy.exp(-2j * numpy.pi * numpy.arange(h) / n)
+    a, b = 0.5 * (1 - 1j * w), 0.5 * (1 + 1j * w)
+    zrev = numpy.roll(zf[..., ::-1], 1, axis=-1)  # Z[(h - k) mod h]
+    out = numpy.empty(x.shape[:-1] + (h + 1,), numpy.complex128)
+    out[..., :h] = zf * a + numpy.conj(zrev) * b
+    out[..., h] = zf[..., 0].real - zf[..., 0].imag
+    return out
+
+
+def irfft_half(xf: numpy.ndarray, threads: int | None = None) -> numpy.ndarray:
+    """Real signals from their half spectra along the last axis through the half-length
+    inverse FFT (examples/demo_specialized_fft.py:82-101; the IRFFT computation
+    :244-331, ``prepare_irfft_input`` of demo_specialized_fft.mako:36-62): the
+    imaginary parts of the first and last bins are ignored, as numpy's irfft does."""
+    xf = numpy.array(xf, numpy.complex128)
+    h = xf.shape[-1] - 1
+    n = 2 * h
+    xf[..., 0] = xf[..., 0].real
+    xf[..., -1] = xf[..., -1].real
+    w = numpy.exp(-2j * numpy.pi * numpy.arange(h) / n)
+    a, b = numpy.conj(0.5 * (1 - 1j * w)), numpy.conj(0.5 * (1 + 1j * w))
+    zf = xf[..., :-1] * a + numpy.conj(xf[..., h:0:-1]) * b
+    z = fft(zf, axes=(zf.ndim - 1,), inverse=True, threads=threads)
+    out = numpy.empty(xf.shape[:-1] + (n,), numpy.float64)
+    out[..., 0::2] = z.real
+    out[..., 1::2] = z.imag
+    return out
+
+
+def aprfft(x: numpy.ndarray, threads: int | None = None) -> numpy.ndarray:
+    """Odd harmonics of real antiperiodic signals (x[k] = -x[N/2 + k]) from their first
+    halves x (..., N/2) -> (..., N/4) (examples/demo_specialized_fft.py:104-121 and the
+    APRFFT computation :379-453): y = x * 4 sin(2 pi n / N), Y = rfft(y), Y *= -i,
+    Y[0] = Y[0] / 2 + 2 sum(x cos(2 pi n / N)), F = cumsum(Y[:-1])."""
+    x = numpy.asarray(x)
+    size = x.shape[-1] * 2
+    n = numpy.arange(size // 2)
+    y = x.astype(numpy.float64) * (4 * numpy.sin(2 * numpy.pi * n / size))
+    yf = rfft_half(y.astype(x.dtype), threads=threads)
+    re1 = 2 * numpy.sum(x.astype(numpy.float64) * numpy.cos(2 * numpy.pi * n / size), axis=-1)
+    yf = yf * -1j
+    yf[..., 0] = yf[..., 0] / 2 + re1
+    return numpy.cumsum(yf[..., :-1], axis=-1)
+
+
+def iaprfft(xf: numpy.ndarray, threads: int | None = None) -> numpy.ndarray:
+    """First halves (..., N/2) of real antiperiodic signals from their N/4 odd harmonics
+    (examples/demo_specialized_fft.py:124-141 and the IAPRFFT computation :456-581):
+    Y[1:-1] = i (F[1:] - F[:-1]), Y[0] = -2 Im F[0], Y[-1] = 2 Im F[-1], y = irfft(Y),
+    x[n] = y[n] / (4 sin(2 pi n / N)) for n >= 1, x[0] = sum(Re F) / (N / 2)."""
+    xf = numpy.asarray(xf, numpy.complex128)
+    q = xf.shape[-1]
+    size = 4 * q
+    yf = numpy.empty(xf.shape[:-1] + (q + 1,), numpy.complex128)
+    yf[..., 1:-1] = 1j * (xf[..., 1:] - xf[..., :-1])
+    yf[..., 0] = -2 * xf[..., 0].imag
+    yf[..., -1] = 2 * xf[..., -1].imag
+    y = irfft_half(yf, threads=threads)
+    out = numpy.empty(xf.shape[:-1] + (size // 2,), numpy.float64)
+    out[..., 1:] = y[..., 1:] / 4 / numpy.sin(2 * numpy.pi * numpy.arange(1, size // 2) / size)
+    out[..., 0] = xf.real.sum(axis=-1) / (size / 2)
+    return out
 
 
 def numpy_ref(x: numpy.ndarray, axes=None, inverse: bool = False) -> numpy.ndarray:

@@ -42,6 +42,8 @@ FLAG_PLANE_WIDE = 8
 FLAG_NO_TMA = 16
 FLAG_PAIR = 32
 FLAG_REAL_POST = 64
+FLAG_REAL_PRE = 128
+FLAG_ANTIPERIODIC = 256
 
 EXPORTED = (
     "rk_edge_init",
@@ -68,6 +70,10 @@ EXPORTED = (
     "rk_rfft_twiddles",
     "rk_rfft_post",
     "rk_irfft_pre",
+    "rk_aprfft_twiddles",
+    "rk_aprfft_twiddle",
+    "rk_aprfft_post",
+    "rk_iaprfft_pre",
 )
 
 I64A = ctypes.c_int64 * MAXD
@@ -172,6 +178,10 @@ def lib() -> ctypes.CDLL:
         L.rk_rfft_twiddles.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, vp]
         L.rk_rfft_post.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, vp]
         L.rk_irfft_pre.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, vp]
+        L.rk_aprfft_twiddles.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, vp]
+        L.rk_aprfft_twiddle.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, vp]
+        L.rk_aprfft_post.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, vp]
+        L.rk_iaprfft_pre.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, vp]
         L.rk_fftshift_execute.argtypes = [
             vp,
             vp,

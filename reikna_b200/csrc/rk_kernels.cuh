@@ -243,6 +243,7 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
     if (f & SF_PRE_CONJ) v = cconj(v);
     if (!(la.ok && a < s.ax_len)) return;
     if (f & SF_CHIRP) v = cmul(v, reinterpret_cast<const V*>(s.chirp)[a]);
+    if (f & SF_TAB) v = cmul(v, reinterpret_cast<const V*>(s.tab)[a]);
     if (f & SF_POST_CONJ) v = cconj(v);
     if (f & SF_SCALE) v = cmul(v, cmk<V>((T)s.scale_re, (T)s.scale_im));
     int64_t u = a + s.ax_shift;
@@ -307,6 +308,33 @@ __device__ __forceinline__ void scale_block(const Side& s, cplx<T>* v) {
 #pragma unroll
         for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
     }
+}
+
+// The value ops of a pass-dtype side without tables, for an element read outside the
+// block load (the Nyquist bin of an inverse real transform).
+template <typename T>
+__device__ __forceinline__ cplx<T> edge_value(const Side& s, cplx<T> v) {
+    if (s.flags & SF_SCALE) {
+        if (s.scale_im == 0.0) {
+            v.x *= (T)s.scale_re;
+            v.y *= (T)s.scale_re;
+        } else {
+            v = cmul(v, cmk<cplx<T>>((T)s.scale_re, (T)s.scale_im));
+        }
+    }
+    if (((s.flags & SF_PRE_CONJ) != 0) != ((s.flags & SF_POST_CONJ) != 0)) v.y = -v.y;
+    return v;
+}
+
+// y A + conj(ym) B with A = h (1 - i w), B = h (1 + i w): the step between a real
+// signal's spectrum and the half-length complex spectrum of its sample pairs
+template <typename T>
+__device__ __forceinline__ cplx<T> real_mix(cplx<T> y, cplx<T> ym, cplx<T> w, T h) {
+    using V = cplx<T>;
+    const V a = cmk<V>(h * (T(1) + w.y), -h * w.x);
+    const V b = cmk<V>(h * (T(1) - w.y), h * w.x);
+    const V x = cmul(y, a), z = cmul(cconj(ym), b);
+    return cmk<V>(x.x + z.x, x.y + z.y);
 }
 
 template <typename T, int N, class PosF>
@@ -423,6 +451,14 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
             for (int i = 0; i < N; ++i) {
                 const int a = a0 + pos(i) * jB;
                 if (a < alen) v[i] = cmul(v[i], __ldg(ch + a));
+            }
+        }
+        if (f & SF_TAB) {
+            const V* tb = reinterpret_cast<const V*>(s.tab);
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int a = a0 + pos(i) * jB;
+                if (a < alen) v[i] = cmul(v[i], __ldg(tb + a));
             }
         }
         if (f & SF_POST_CONJ) {
@@ -574,6 +610,37 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
     {
         const LineAddr la = line_addr(p.ld, line, p.C, p.I, lok);
         load_block<T, RT>(p.ld, la, [&](int i) { return E::in_pos(tb, i / R0, i % R0); }, v);
+        if constexpr (VAR == 4) {
+            // half-length spectrum of a real signal from its bins y (the inverse real
+            // transforms; y arrives conjugated, as the inverse FFT's first load):
+            // y[k] A_k + conj(y[mirror k]) B_k; with rnyq the mirror of bin 0 is bin L
+            // of the input row, and bins 0 and L lose their imaginary parts
+            static_assert(MODE == MODE_POS, "the real-signal step needs whole lines");
+            V yl = cmk<V>(T(0), T(0));
+            if (p.rnyq && la.ok) yl = edge_value<T>(p.ld, reinterpret_cast<const V*>(p.ld.ptr)[la.base + (int64_t)L * p.ld.ax_stride]);
+#pragma unroll
+            for (int z = 0; z < RT / R0; ++z)
+#pragma unroll
+                for (int m = 0; m < R0; ++m) sm[E::sidx(ln, E::in_pos(tb, z, m))] = v[z * R0 + m];
+            __syncthreads();
+            const V* wk = reinterpret_cast<const V*>(p.rmix);
+            const T h = (T)p.rh;
+#pragma unroll
+            for (int z = 0; z < RT / R0; ++z)
+#pragma unroll
+                for (int m = 0; m < R0; ++m) {
+                    const int k = E::in_pos(tb, z, m);
+                    V yk = v[z * R0 + m];
+                    V ym = sm[E::sidx(ln, (L - k - p.rodd) & (L - 1))];
+                    if (p.rnyq && k == 0) {
+                        ym = yl;
+                        yk.y = T(0);
+                        ym.y = T(0);
+                    }
+                    v[z * R0 + m] = real_mix<T>(yk, ym, __ldg(wk + k), h);
+                }
+            __syncthreads();
+        }
     }
     E::run(v, sm, ln, tb, tw);
     if constexpr (VAR == 1) {
@@ -597,32 +664,27 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
     }
     if constexpr (VAR == 3) {
         // real-signal spectrum from the half-length spectrum Z of this line (the line
-        // holds x[2n] + i x[2n+1]): X[k] = Z[k] A[k] + conj(Z[(L - k) mod L]) B[k],
-        // A = (1 - i W^k) / 2, B = (1 + i W^k) / 2, W = exp(-2 pi i / 2L), with W^k from
-        // the plan's FP64-generated table in st.tab; st.post_param = 1 also stores
-        // X[L] = Re Z[0] - Im Z[0] (the Nyquist bin) after the line's L positions
+        // holds x[2n] + i x[2n+1]): X[k] = Z[k] A_k + conj(Z[mirror k]) B_k with the
+        // plan's FP64-generated w_k in rmix; with rnyq the Nyquist bin
+        // X[L] = Re Z[0] - Im Z[0] is stored after the line's L positions
         static_assert(MODE == MODE_POS, "the real-spectrum step needs whole lines");
 #pragma unroll
         for (int z = 0; z < RT / RL; ++z)
 #pragma unroll
             for (int m = 0; m < RL; ++m) sm[E::sidx(ln, E::out_pos(tb, z, m))] = v[z * RL + m];
         __syncthreads();
-        const V* wk = reinterpret_cast<const V*>(p.st.tab);
+        const V* wk = reinterpret_cast<const V*>(p.rmix);
+        const T h = (T)p.rh;
 #pragma unroll
         for (int z = 0; z < RT / RL; ++z)
 #pragma unroll
             for (int m = 0; m < RL; ++m) {
                 const int k = E::out_pos(tb, z, m);
-                const V zk = sm[E::sidx(ln, k)];
-                const V zc = cconj(sm[E::sidx(ln, (L - k) & (L - 1))]);
-                const V w = __ldg(wk + k);
-                const V a = cmk<V>(T(0.5) * (T(1) + w.y), T(-0.5) * w.x);
-                const V bb = cmk<V>(T(0.5) * (T(1) - w.y), T(0.5) * w.x);
-                const V x = cmul(zk, a), y = cmul(zc, bb);
-                v[z * RL + m] = cmk<V>(x.x + y.x, x.y + y.y);
+                v[z * RL + m] = real_mix<T>(sm[E::sidx(ln, k)], sm[E::sidx(ln, (L - k - p.rodd) & (L - 1))],
+                                            __ldg(wk + k), h);
             }
         const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
-        if (tb == 0 && la.ok && p.st.post_param == 1.0) {
+        if (tb == 0 && la.ok && p.rnyq) {
             const V z0 = sm[E::sidx(ln, 0)];
             V xl = cmk<V>(z0.x - z0.y, T(0));
             if (p.st.flags & SF_SCALE) xl = cmul(xl, cmk<V>((T)p.st.scale_re, (T)p.st.scale_im));

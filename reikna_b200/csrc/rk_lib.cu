@@ -181,6 +181,17 @@ __global__ void k_gen_rpost(int64_t L, float2* f, double2* d) {
     if (d) d[k] = make_double2(c, s);
 }
 
+// exp(-i pi (2k + 1) / 2L), k = 0 .. L - 1, for the odd-harmonic step of the
+// antiperiodic real transforms (RK_FLAG_ANTIPERIODIC)
+__global__ void k_gen_rodd(int64_t L, float2* f, double2* d) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= L) return;
+    double s, c;
+    sincospi(-(double)(2 * k + 1) / (double)(2 * L), &s, &c);
+    if (f) f[k] = make_float2((float)c, (float)s);
+    if (d) d[k] = make_double2(c, s);
+}
+
 // von Hann window 0.5 (1 - cos(2 pi u / (w - 1))), u < w, in FP64, rounded once
 __global__ void k_gen_window(int32_t w, float* f, double* d) {
     const int32_t u = blockIdx.x * blockDim.x + threadIdx.x;
@@ -271,8 +282,17 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
     axes.erase(std::remove_if(axes.begin(), axes.end(), [&](int a) { return d.shape[a] == 1; }), axes.end());
 
     const int nd = d.ndim;
-    if ((d.flags & RK_FLAG_REAL_POST) && (d.naxes != 1 || d.axes[0] != nd - 1 || d.shape[nd - 1] < 8)) {
-        set_error("RK_FLAG_REAL_POST needs a transform of the last axis only, of at least 8 points");
+    const int32_t real_flags = d.flags & (RK_FLAG_REAL_POST | RK_FLAG_REAL_PRE);
+    if (real_flags == (RK_FLAG_REAL_POST | RK_FLAG_REAL_PRE)) {
+        set_error("RK_FLAG_REAL_POST and RK_FLAG_REAL_PRE exclude each other");
+        return RK_ERR_INVALID;
+    }
+    if ((d.flags & RK_FLAG_ANTIPERIODIC) && !real_flags) {
+        set_error("RK_FLAG_ANTIPERIODIC needs RK_FLAG_REAL_POST or RK_FLAG_REAL_PRE");
+        return RK_ERR_INVALID;
+    }
+    if (real_flags && (d.naxes != 1 || d.axes[0] != nd - 1 || d.shape[nd - 1] < 8)) {
+        set_error("a one-pass real transform needs a transform of the last axis only, of at least 8 points");
         return RK_ERR_UNSUPPORTED;
     }
     int cur = SB_IN;
@@ -352,8 +372,9 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
                     d.output.strides[ax - 1] == 1 && d.shape[ax - 1] > 1)
                     p.var = 2;
                 // the real-signal spectrum step fused into the store (RK_FLAG_REAL_POST)
-                if ((d.flags & RK_FLAG_REAL_POST) && I == 1 && last_axis && n >= 8 && n <= (dbl ? 4096 : 8192))
-                    p.var = 3;
+                // or into the load (RK_FLAG_REAL_PRE)
+                if (real_flags && I == 1 && last_axis && n >= 8 && n <= (dbl ? 4096 : 8192))
+                    p.var = (d.flags & RK_FLAG_REAL_POST) ? 3 : 4;
                 p.axis = ax;
                 p.O = O; p.C = 1; p.I = I;
                 p.ld.buf = cur; p.ld.ax_len = n; p.ld.cA = 0; p.ld.jB = 1;
@@ -481,12 +502,22 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
             }
         }
     }
-    if (d.flags & RK_FLAG_REAL_POST) {
+    if (real_flags) {
         const int ax = nd - 1;
-        if (d.naxes != 1 || d.axes[0] != ax || P.passes.size() != 1 || P.passes[0].var != 3 ||
-            d.output.strides[ax] != 1 || (d.output.shape[ax] != d.shape[ax] && d.output.shape[ax] != d.shape[ax] + 1)) {
-            set_error("RK_FLAG_REAL_POST needs a one-pass forward transform of the last axis (a power of two of "
-                      "8 to 8192 points, 4096 for complex128) with a contiguous output of L or L + 1 bins");
+        const bool ap = d.flags & RK_FLAG_ANTIPERIODIC;
+        const bool post = d.flags & RK_FLAG_REAL_POST;
+        const rk_edge& spec = post ? d.output : d.input;  // the edge holding the real signal's bins
+        const int64_t L = d.shape[ax];
+        const bool bins_ok = ap ? spec.shape[ax] == L
+                                : (post ? (spec.shape[ax] == L || spec.shape[ax] == L + 1) : spec.shape[ax] == L + 1);
+        if (P.passes.size() != 1 || P.passes[0].var != (post ? 3 : 4) || spec.strides[ax] != 1 || !bins_ok ||
+            spec.shift[ax] != 0 || (!post && d.output.shape[ax] != L)) {
+            set_error(post ? "RK_FLAG_REAL_POST needs a one-pass transform of the last axis (a power of two of 8 to "
+                             "8192 points, 4096 for complex128) with a contiguous output of L or L + 1 bins (L with "
+                             "RK_FLAG_ANTIPERIODIC)"
+                           : "RK_FLAG_REAL_PRE needs a one-pass transform of the last axis (a power of two of 8 to "
+                             "8192 points, 4096 for complex128) with a contiguous input of L + 1 bins (L with "
+                             "RK_FLAG_ANTIPERIODIC) and an output of L pairs");
             return RK_ERR_UNSUPPORTED;
         }
     }
@@ -1004,6 +1035,10 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         pp.nlines = ps.O * ps.C * ps.I;
         build_side(*desc, ps.ld, ps.axis, dbl, true, pp.ld);
         build_side(*desc, ps.st, ps.kind == PK_PLANE ? ps.axis2 : ps.axis, dbl, false, pp.st);
+        // antiperiodic transforms: W_2L^m on the first load (forward) or, conjugated
+        // by the inverse's last conjugation, on the last store
+        const bool ap_tab = (ps.var == 3 || ps.var == 4) && (desc->flags & RK_FLAG_ANTIPERIODIC);
+        if (ap_tab) (ps.var == 3 ? pp.ld : pp.st).flags |= SF_TAB;
         mark_fast(pp.ld, dbl, ps.kind == PK_PLANE ? ps.L2 : ps.L);
         mark_fast(pp.st, dbl, ps.kind == PK_PLANE ? ps.L1 : ps.L);
         mark_fast2(pp.ld, dbl, ps.kind == PK_PLANE ? ps.L2 : ps.L, ps.C);
@@ -1023,19 +1058,40 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             mark_fastr(pp.ld, dbl, ps.L, true);
             mark_fastr(pp.st, dbl, ps.L, false);
         }
-        if (ps.var == 3) {
-            if (pp.st.fmt != (dbl ? RK_FMT_C128 : RK_FMT_C64)) {
-                set_error("RK_FLAG_REAL_POST needs a complex output of the transform's precision");
+        if (ps.var == 3 || ps.var == 4) {
+            const int cfmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
+            if (pp.st.fmt != cfmt || pp.ld.fmt != cfmt) {
+                set_error("a one-pass real transform needs complex edges of the transform's precision");
                 return fail(RK_ERR_UNSUPPORTED);
             }
+            const bool ap = desc->flags & RK_FLAG_ANTIPERIODIC;
+            const int64_t L = ps.L;
+            const int esz = dbl ? 16 : 8;
             void* wt = nullptr;
-            const int trc = alloc((int64_t)(ps.L + 1) * (dbl ? 16 : 8), &wt);
+            const int trc = alloc((L + 1) * esz, &wt);
             if (trc) return fail(trc);
-            k_gen_rpost<<<(unsigned)((ps.L + 256) / 256), 256>>>(ps.L, dbl ? nullptr : (float2*)wt,
+            if (ap)
+                k_gen_rodd<<<(unsigned)((L + 255) / 256), 256>>>(L, dbl ? nullptr : (float2*)wt,
                                                                  dbl ? (double2*)wt : nullptr);
+            else
+                k_gen_rpost<<<(unsigned)((L + 256) / 256), 256>>>(L, dbl ? nullptr : (float2*)wt,
+                                                                  dbl ? (double2*)wt : nullptr);
             CK(cudaGetLastError());
-            pp.st.tab = wt;
-            pp.st.post_param = desc->output.shape[ps.axis] > ps.L ? 1.0 : 0.0;
+            pp.rmix = wt;
+            pp.rodd = ap ? 1 : 0;
+            // forward: 2 (Z A + conj(Z') B) for the odd harmonics (the doubled half
+            // period); inverse: one half of the forward's A, B (a quarter for them)
+            pp.rh = ps.var == 3 ? (ap ? 1.0 : 0.5) : (ap ? 0.25 : 0.5);
+            pp.rnyq = ap ? 0 : (ps.var == 4 ? 1 : (desc->output.shape[ps.axis] > L ? 1 : 0));
+            if (ap_tab) {
+                void* tt = nullptr;
+                const int rc2 = alloc((L + 1) * esz, &tt);
+                if (rc2) return fail(rc2);
+                k_gen_rpost<<<(unsigned)((L + 256) / 256), 256>>>(L, dbl ? nullptr : (float2*)tt,
+                                                                  dbl ? (double2*)tt : nullptr);
+                CK(cudaGetLastError());
+                (ps.var == 3 ? pp.ld : pp.st).tab = tt;
+            }
         }
         if (ps.ld.chirp_axis >= 0) {
             auto& bt = blue_tabs[ps.ld.chirp_axis];
@@ -1342,6 +1398,10 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
     cudaStream_t st = (cudaStream_t)stream;
     if (plan && inverse && (plan->desc.flags & RK_FLAG_REAL_POST)) {
         set_error("a plan with RK_FLAG_REAL_POST runs forward only");
+        return RK_ERR_INVALID;
+    }
+    if (plan && !inverse && (plan->desc.flags & RK_FLAG_REAL_PRE)) {
+        set_error("a plan with RK_FLAG_REAL_PRE runs inverse only");
         return RK_ERR_INVALID;
     }
     std::vector<PassParams> prm;

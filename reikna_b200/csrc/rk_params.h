@@ -76,6 +76,14 @@ struct PassParams {
     int64_t tw4_N;        // four-step twiddle modulus (power of two <= 2^24)
     const void* blue_k;   // Bluestein kernel spectrum (fused single-pass kernel)
     int32_t* status;
+    // real-signal step of a one-pass real transform, after the FFT of a last pass
+    // (var 3) or before the FFT of a first pass (var 4): y[k] A_k + conj(y[mirror k])
+    // B_k with A_k = rh (1 - i w_k), B_k = rh (1 + i w_k), w_k = rmix[k], and
+    // mirror k = (L - k - rodd) mod L; rnyq: the bin L is also stored (var 3) or
+    // read as the mirror of bin 0 (var 4)
+    const void* rmix;
+    double rh;
+    int32_t rodd, rnyq;
 };
 
 // Clustered two-axis pass: axis r (rows, length L1) and the contiguous axis q

@@ -98,6 +98,68 @@ __global__ void k_irfft_pre(V* __restrict__ z, const V* __restrict__ x, const V*
     }
 }
 
+// Antiperiodic real signals (x[n + 2L] = -x[n], length 4L, first half x[0 .. 2L)):
+// only the odd harmonics F[k] = X[2k + 1], k < L, are non-zero, and with
+// c[m] = (x[2m] + i x[2m+1]) W_2L^m, C = FFT_L(c), w_k = exp(-i pi (2k + 1) / 2L):
+//     F[k] = C[k] (1 - i w_k) + conj(C[L - 1 - k]) (1 + i w_k),
+//     C[k] = (F[k] conj(1 - i w_k) + conj(F[L - 1 - k]) conj(1 + i w_k)) / 4,
+// the second inverting the first pairwise (k, L - 1 - k).  The table holds w_k for
+// k < L followed by W_2L^m for m < L.
+template <typename V>
+__global__ void k_aprfft_twiddles(V* t, int64_t half) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= half) return;
+    double s, c;
+    sincospi(-(double)(2 * k + 1) / (double)(2 * half), &s, &c);
+    t[k] = mk<V>((typename Real<V>::T)c, (typename Real<V>::T)s);
+    sincospi(-(double)k / (double)half, &s, &c);
+    t[half + k] = mk<V>((typename Real<V>::T)c, (typename Real<V>::T)s);
+}
+
+template <typename V>
+__global__ void k_aprfft_post(V* __restrict__ out, const V* __restrict__ z, const V* __restrict__ w, int64_t half,
+                              int64_t batch) {
+    using T = typename Real<V>::T;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        const V* zr = z + b * half;
+        V* orow = out + b * half;
+        for (int64_t k = threadIdx.x; k < half; k += blockDim.x) {
+            const V wk = __ldg(w + k);
+            const V x = mulc(zr[k], mk<V>(T(1) + wk.y, -wk.x));
+            const V y = mulc(conjc(zr[half - 1 - k]), mk<V>(T(1) - wk.y, wk.x));
+            orow[k] = mk<V>(x.x + y.x, x.y + y.y);
+        }
+    }
+}
+
+template <typename V>
+__global__ void k_iaprfft_pre(V* __restrict__ z, const V* __restrict__ x, const V* __restrict__ w, int64_t half,
+                              int64_t batch) {
+    using T = typename Real<V>::T;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        const V* xr = x + b * half;
+        V* zr = z + b * half;
+        for (int64_t k = threadIdx.x; k < half; k += blockDim.x) {
+            const V wk = __ldg(w + k);
+            const V p = mulc(xr[k], mk<V>(T(0.25) * (T(1) + wk.y), T(0.25) * wk.x));
+            const V q = mulc(conjc(xr[half - 1 - k]), mk<V>(T(0.25) * (T(1) - wk.y), T(-0.25) * wk.x));
+            zr[k] = mk<V>(p.x + q.x, p.y + q.y);
+        }
+    }
+}
+
+// rows times W_2L^m (inverse: its conjugate); in place allowed
+template <typename V>
+__global__ void k_aprfft_twiddle(V* out, const V* in, const V* t, int64_t half, int64_t batch, int inverse) {
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        for (int64_t m = threadIdx.x; m < half; m += blockDim.x) {
+            V tm = __ldg(t + m);
+            if (inverse) tm = conjc(tm);
+            out[b * half + m] = mulc(in[b * half + m], tm);
+        }
+    }
+}
+
 // CTAs for a row-per-CTA kernel: the rows, at most 16 waves of one CTA per SM
 int grid_for(int64_t rows) {
     static int nsm = 0;
@@ -188,4 +250,78 @@ extern "C" int rk_irfft_pre(void* z, const void* x, const void* table, int32_t f
     else
         k_irfft_pre<double2><<<g, 256, 0, st>>>((double2*)z, (const double2*)x, (const double2*)table, half, batch);
     return finish("rk_irfft_pre");
+}
+
+extern "C" int rk_aprfft_twiddles(void* table, int32_t fmt, int64_t half, void* stream) {
+    if (int rc = check_fmt(fmt, "rk_aprfft_twiddles")) return rc;
+    if (!table || half < 1) {
+        set_error("rk_aprfft_twiddles: null table or half length < 1");
+        return RK_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned g = (unsigned)((half + 255) / 256);
+    if (fmt == RK_FMT_C64)
+        k_aprfft_twiddles<float2><<<g, 256, 0, st>>>((float2*)table, half);
+    else
+        k_aprfft_twiddles<double2><<<g, 256, 0, st>>>((double2*)table, half);
+    return finish("rk_aprfft_twiddles");
+}
+
+extern "C" int rk_aprfft_post(void* out, const void* z, const void* table, int32_t fmt, int64_t half, int64_t batch,
+                              void* stream) {
+    if (int rc = check_fmt(fmt, "rk_aprfft_post")) return rc;
+    if (!out || !z || !table || half < 1 || batch < 1) {
+        set_error("rk_aprfft_post: null pointer or non-positive size");
+        return RK_ERR_INVALID;
+    }
+    if (out == z) {
+        set_error("rk_aprfft_post: output may not alias the half-length spectrum");
+        return RK_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int g = grid_for(batch);
+    if (fmt == RK_FMT_C64)
+        k_aprfft_post<float2><<<g, 256, 0, st>>>((float2*)out, (const float2*)z, (const float2*)table, half, batch);
+    else
+        k_aprfft_post<double2><<<g, 256, 0, st>>>((double2*)out, (const double2*)z, (const double2*)table, half, batch);
+    return finish("rk_aprfft_post");
+}
+
+extern "C" int rk_iaprfft_pre(void* z, const void* x, const void* table, int32_t fmt, int64_t half, int64_t batch,
+                              void* stream) {
+    if (int rc = check_fmt(fmt, "rk_iaprfft_pre")) return rc;
+    if (!z || !x || !table || half < 1 || batch < 1) {
+        set_error("rk_iaprfft_pre: null pointer or non-positive size");
+        return RK_ERR_INVALID;
+    }
+    if (z == x) {
+        set_error("rk_iaprfft_pre: output may not alias the harmonics");
+        return RK_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int g = grid_for(batch);
+    if (fmt == RK_FMT_C64)
+        k_iaprfft_pre<float2><<<g, 256, 0, st>>>((float2*)z, (const float2*)x, (const float2*)table, half, batch);
+    else
+        k_iaprfft_pre<double2><<<g, 256, 0, st>>>((double2*)z, (const double2*)x, (const double2*)table, half, batch);
+    return finish("rk_iaprfft_pre");
+}
+
+extern "C" int rk_aprfft_twiddle(void* out, const void* in, const void* table, int32_t fmt, int64_t half,
+                                 int64_t batch, int32_t inverse, void* stream) {
+    if (int rc = check_fmt(fmt, "rk_aprfft_twiddle")) return rc;
+    if (!out || !in || !table || half < 1 || batch < 1) {
+        set_error("rk_aprfft_twiddle: null pointer or non-positive size");
+        return RK_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int g = grid_for(batch);
+    // the table's second half holds W_2L^m
+    if (fmt == RK_FMT_C64)
+        k_aprfft_twiddle<float2><<<g, 256, 0, st>>>((float2*)out, (const float2*)in, (const float2*)table + half, half,
+                                                    batch, inverse ? 1 : 0);
+    else
+        k_aprfft_twiddle<double2><<<g, 256, 0, st>>>((double2*)out, (const double2*)in, (const double2*)table + half,
+                                                     half, batch, inverse ? 1 : 0);
+    return finish("rk_aprfft_twiddle");
 }

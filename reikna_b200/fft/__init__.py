@@ -1,5 +1,5 @@
 from .fft import FFT
 from .fftshift import FFTShift
-from .rfft import IRFFT, RFFT
+from .rfft import APRFFT, IAPRFFT, IRFFT, RFFT
 
-__all__ = ["FFT", "FFTShift", "RFFT", "IRFFT"]
+__all__ = ["FFT", "FFTShift", "RFFT", "IRFFT", "APRFFT", "IAPRFFT"]

@@ -116,3 +116,148 @@ def test_fused_rfft_is_one_launch(shape, dtype):
         ref = numpy.fft.rfft(x.astype(numpy.float64))[..., : spec.shape[-1]]
         ctype = numpy.complex64 if dtype == numpy.float32 else numpy.complex128
         assert rel_l2(spec.cpu().numpy(), ref) < fft_bound(ctype, n)
+
+
+def test_oracle_real_transforms_match_numpy():
+    """The oracle's restatement of the example's reference functions agrees with numpy,
+    as the example's own tests require (demo_specialized_fft.py:627-705)."""
+    from oracle import oracle
+
+    rng = numpy.random.default_rng(64)
+    for dt in (numpy.float32, numpy.float64):
+        half = rng.standard_normal((3, 512)).astype(dt)
+        full = numpy.concatenate([half, -half], axis=-1).astype(numpy.float64)
+        ref = numpy.fft.rfft(full)[:, 1::2]
+        assert numpy.allclose(oracle.aprfft(half), ref, atol=1e-4, rtol=1e-4)
+        f = (rng.standard_normal((3, 256)) + 1j * rng.standard_normal((3, 256))).astype(numpy.complex128)
+        spec = numpy.zeros((3, 513), numpy.complex128)
+        spec[:, 1::2] = f
+        assert numpy.allclose(oracle.iaprfft(f), numpy.fft.irfft(spec)[:, :512], atol=1e-4, rtol=1e-4)
+        x = rng.standard_normal((2, 1000)).astype(dt)
+        assert numpy.allclose(oracle.rfft_half(x), numpy.fft.rfft(x.astype(numpy.float64)), atol=1e-4, rtol=1e-4)
+        back = oracle.irfft_half(numpy.fft.rfft(x.astype(numpy.float64)))
+        assert numpy.allclose(back, x, atol=1e-4, rtol=1e-4)
+
+
+def test_antiperiodic_signatures_and_errors():
+    from reikna_b200.core import ArrayMetadata
+    from reikna_b200.fft import APRFFT, IAPRFFT
+
+    a = APRFFT(ArrayMetadata((8, 512), numpy.float32))
+    assert tuple(a.parameter.output.shape) == (8, 256) and a.parameter.output.dtype == numpy.complex64
+    i = IAPRFFT(ArrayMetadata((8, 256), numpy.complex128))
+    assert tuple(i.parameter.output.shape) == (8, 512) and i.parameter.output.dtype == numpy.float64
+    with pytest.raises(ValueError):
+        APRFFT(ArrayMetadata((8, 511), numpy.float32))
+    with pytest.raises(ValueError):
+        APRFFT(ArrayMetadata((8, 512), numpy.complex64))
+    with pytest.raises(ValueError):
+        IAPRFFT(ArrayMetadata((8, 256), numpy.float32))
+
+
+def test_real_pre_and_antiperiodic_flags_plan_one_pass():
+    from reikna_b200 import _native as N
+
+    cases = [(N.FLAG_REAL_PRE, 513, 512, 4), (N.FLAG_REAL_POST | N.FLAG_ANTIPERIODIC, 512, 512, 3),
+             (N.FLAG_REAL_PRE | N.FLAG_ANTIPERIODIC, 512, 512, 4)]
+    for flags, n_in, n_out, var in cases:
+        d = N.desc(N.FMT_C64, (64, 512), (1,), flags)
+        d.input = N.edge(N.FMT_C64, (64, n_in))
+        d.output = N.edge(N.FMT_C64, (64, n_out))
+        plan = N.describe(d)
+        assert len(plan["passes"]) == 1 and plan["passes"][0]["var"] == var
+    # the inverse reads L + 1 bins, the antiperiodic transforms L harmonics
+    for flags, n_in, n_out in [(N.FLAG_REAL_PRE, 512, 512), (N.FLAG_REAL_POST | N.FLAG_ANTIPERIODIC, 512, 513),
+                               (N.FLAG_REAL_PRE | N.FLAG_ANTIPERIODIC, 513, 512)]:
+        d = N.desc(N.FMT_C64, (64, 512), (1,), flags)
+        d.input = N.edge(N.FMT_C64, (64, n_in))
+        d.output = N.edge(N.FMT_C64, (64, n_out))
+        with pytest.raises(NotImplementedError):
+            N.describe(d)
+    for flags in (N.FLAG_ANTIPERIODIC, N.FLAG_REAL_POST | N.FLAG_REAL_PRE):
+        with pytest.raises(ValueError):
+            N.describe(N.desc(N.FMT_C64, (64, 512), (1,), flags))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize(
+    "shape,dtype",
+    [((512,), numpy.float32), ((64, 1024), numpy.float32), ((3, 8192), numpy.float64), ((2, 16), numpy.float32),
+     ((5, 1000), numpy.float32), ((2, 65536), numpy.float32), ((3, 600), numpy.float64)],
+)
+def test_aprfft_and_iaprfft(shape, dtype):
+    """Against the oracle's restatement of the reference (atol = rtol = 1e-4, the example's
+    own tolerance) and numpy in FP64 (the rel-L2 bound); the last three shapes have half
+    lengths without a one-pass plan (Bluestein, four-step) and take the multi-kernel route."""
+    import torch
+
+    from oracle import oracle
+    from reikna_b200.fft import APRFFT, IAPRFFT
+
+    rng = numpy.random.default_rng(65)
+    x = rng.standard_normal(shape).astype(dtype)
+    ctype = numpy.complex64 if dtype == numpy.float32 else numpy.complex128
+    cdt = torch.complex64 if dtype == numpy.float32 else torch.complex128
+    n = shape[-1]
+    t = torch.from_numpy(x).cuda()
+    harm = torch.empty(shape[:-1] + (n // 2,), dtype=cdt, device="cuda")
+    fwd = APRFFT(t).compile()
+    fused = (n // 2) in [2**k for k in range(3, 14 if dtype == numpy.float32 else 13)]
+    assert (fwd.launches == 1) == fused
+    fwd(None, harm, t)
+    back = torch.empty_like(t)
+    inv = IAPRFFT(harm).compile()
+    assert (inv.launches == 1) == fused
+    inv(None, back, harm)
+    torch.cuda.synchronize()
+    got = harm.cpu().numpy()
+    full = numpy.concatenate([x, -x], axis=-1).astype(numpy.float64)
+    ref = numpy.fft.rfft(full, axis=-1)[..., 1::2]
+    assert rel_l2(got, ref) < fft_bound(ctype, 2 * n)
+    orc = oracle.aprfft(x)
+    assert numpy.allclose(got, orc, atol=1e-4 * max(1.0, numpy.abs(orc).max()), rtol=1e-4)
+    y = back.cpu().numpy()
+    assert rel_l2(y, x.astype(numpy.float64)) < 2 * fft_bound(ctype, 2 * n)
+    assert numpy.allclose(y, oracle.iaprfft(got.astype(numpy.complex128)), atol=1e-4, rtol=1e-4)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,dtype", [((16384, 1024), numpy.float32), ((4, 16384), numpy.float32), ((3, 8192), numpy.float64)])
+def test_fused_irfft_is_one_launch(shape, dtype):
+    import torch
+
+    from reikna_b200.fft import IRFFT
+
+    rng = numpy.random.default_rng(66)
+    n = shape[-1]
+    ctype = numpy.complex64 if dtype == numpy.float32 else numpy.complex128
+    spec = numpy.fft.rfft(rng.uniform(-1, 1, shape)).astype(ctype)
+    spec[..., 0] += 0.5j  # ignored, as numpy's irfft ignores it
+    s = torch.from_numpy(spec).cuda()
+    out = torch.empty(shape, dtype=torch.float32 if dtype == numpy.float32 else torch.float64, device="cuda")
+    c = IRFFT(s).compile()
+    assert c.launches == 1
+    c(None, out, s)
+    torch.cuda.synchronize()
+    ref = numpy.fft.irfft(spec.astype(numpy.complex128), n=n, axis=-1)
+    assert rel_l2(out.cpu().numpy(), ref) < fft_bound(ctype, n)
+
+
+@pytest.mark.gpu
+def test_real_plans_run_in_their_direction_only():
+    import torch
+
+    from reikna_b200 import _native as N
+
+    for flags, n_in, wrong in [(N.FLAG_REAL_POST, 256, 1), (N.FLAG_REAL_PRE, 257, 0),
+                               (N.FLAG_REAL_POST | N.FLAG_ANTIPERIODIC, 256, 1), (N.FLAG_REAL_PRE | N.FLAG_ANTIPERIODIC, 256, 0)]:
+        d = N.desc(N.FMT_C64, (4, 256), (1,), flags)
+        d.input = N.edge(N.FMT_C64, (4, n_in))
+        d.output = N.edge(N.FMT_C64, (4, 256))
+        plan = N.Plan(d)
+        a = torch.zeros((4, n_in), dtype=torch.complex64, device="cuda")
+        b = torch.zeros((4, 256), dtype=torch.complex64, device="cuda")
+        with pytest.raises(ValueError):
+            plan.execute([b.data_ptr()], [a.data_ptr()], inverse=wrong, stream=0)
+        plan.execute([b.data_ptr()], [a.data_ptr()], inverse=1 - wrong, stream=0)
+    torch.cuda.synchronize()
