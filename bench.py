@@ -798,6 +798,149 @@ def run_precision(args, rank: int, world: int, local_rank: int) -> int:
     return 0
 
 
+# --- next rows: spectrogram, FFTShift, Transpose, real transforms ------------------
+
+
+def run_next(args, rank: int, world: int, local_rank: int) -> int:
+    """The computations around the FFT at their workload sizes, each through its public
+    computation API: the spectrogram of a 2^22-sample float32 signal (Hann 1024, hop
+    256; frame-major and transposed), FFTShift and Transpose of 4096 x 4096 complex64,
+    and the half-length real transforms of 16384 rows of 1024 float32 samples (RFFT,
+    IRFFT, APRFFT, IAPRFFT).  Two buffer sets alternate (each op moves more than the
+    126 MB L2 in total per pair of steps, and the big ones more than L2 per step);
+    device time from CUDA events over the timed steps."""
+    import numpy
+    import torch
+
+    from reikna_b200.algorithms import Transpose
+    from reikna_b200.fft import APRFFT, FFTShift, IAPRFFT, IRFFT, RFFT
+    from reikna_b200.spectrogram import frames, spectrogram
+
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    peak, peak_kind = peaks()
+    rng = numpy.random.default_rng(9)
+    steps = max(1, min(args.steps, 500))
+
+    def timed(call, pairs):
+        for k in range(max(3, args.warmup)):
+            call(*pairs[k % 2])
+        torch.cuda.synchronize(dev)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for k in range(steps):
+            call(*pairs[k % 2])
+        s1.record()
+        torch.cuda.synchronize(dev)
+        return s0.elapsed_time(s1) / steps
+
+    def entry(us, b_alg, err, launches):
+        gbs = b_alg / (us / 1e6) / 1e9
+        return {"us": us, "gbs": gbs, "hbm_frac": gbs / peak, "bytes_algorithmic": b_alg,
+                "rel_l2_vs_fp64": err, "launches": launches}
+
+    def rel(a, b):
+        a = numpy.asarray(a, numpy.complex128)
+        b = numpy.asarray(b, numpy.complex128)
+        return float(numpy.linalg.norm((a - b).ravel()) / numpy.linalg.norm(b.ravel()))
+
+    res = {}
+    # spectrogram: 2^22 samples, N(0,1) plus 8 sinusoids
+    n_sig, nfft, hop = 2**22, 1024, 256
+    t_idx = numpy.arange(n_sig)
+    sig = rng.standard_normal(n_sig)
+    for _ in range(8):
+        sig += rng.uniform(0.1, 2) * numpy.sin(2 * numpy.pi * rng.uniform(0, 0.5) * t_idx + rng.uniform(0, 2 * numpy.pi))
+    sig = sig.astype(numpy.float32)
+    nfr = frames(n_sig, nfft, hop)
+    idx = numpy.arange(nfr)[:, None] * hop + numpy.arange(nfft)[None, :]
+    win = 0.5 * (1 - numpy.cos(2 * numpy.pi * numpy.arange(nfft) / (nfft - 1)))
+    spec_ref = numpy.abs(numpy.fft.rfft(sig.astype(numpy.float64)[idx] * win, axis=1))
+    sigs = [torch.from_numpy(sig).to(dev) for _ in range(2)]
+    for label, transposed in (("spectrogram", False), ("spectrogram_transposed", True)):
+        cc = spectrogram(n_sig, nfft, hop, transposed=transposed).compile(dev)
+        shape = (nfft // 2 + 1, nfr) if transposed else (nfr, nfft // 2 + 1)
+        outs = [torch.empty(shape, dtype=torch.float32, device=dev) for _ in range(2)]
+        us = timed(lambda o, i: cc(None, o, i), list(zip(outs, sigs))) * 1e3
+        got = outs[0].cpu().numpy()
+        res[label] = entry(us, n_sig * 4 + nfr * (nfft // 2 + 1) * 4, rel(got.T if transposed else got, spec_ref),
+                           cc.launches)
+    del spec_ref, idx
+    # FFTShift and Transpose of 4096 x 4096 complex64 (134 MB each way)
+    x = (rng.standard_normal((4096, 4096)) + 1j * rng.standard_normal((4096, 4096))).astype(numpy.complex64)
+    xs = [torch.from_numpy(x).to(dev) for _ in range(2)]
+    ys = [torch.empty_like(xs[0]) for _ in range(2)]
+    cc = FFTShift(xs[0]).compile(dev)
+    us = timed(lambda o, i: cc(None, o, i), list(zip(ys, xs))) * 1e3
+    res["fftshift_4096x4096"] = entry(us, 2 * x.nbytes, rel(ys[0].cpu().numpy(), numpy.fft.fftshift(x)), cc.launches)
+    cc = Transpose(xs[0]).compile(dev)
+    us = timed(lambda o, i: cc(None, o, i), list(zip(ys, xs))) * 1e3
+    res["transpose_4096x4096"] = entry(us, 2 * x.nbytes, rel(ys[0].cpu().numpy(), x.T), cc.launches)
+    del x, xs, ys
+    # real transforms: 16384 x 1024 float32
+    shape = (16384, 1024)
+    xr = rng.uniform(-1, 1, shape).astype(numpy.float32)
+    full = numpy.fft.rfft(xr.astype(numpy.float64), axis=1)
+    harm = numpy.fft.rfft(numpy.concatenate([xr, -xr], axis=1).astype(numpy.float64), axis=1)[:, 1::2]
+    xrs = [torch.from_numpy(xr).to(dev) for _ in range(2)]
+    specs = [torch.empty((16384, 513), dtype=torch.complex64, device=dev) for _ in range(2)]
+    hs = [torch.empty((16384, 512), dtype=torch.complex64, device=dev) for _ in range(2)]
+    backs = [torch.empty_like(xrs[0]) for _ in range(2)]
+    for label, comp, outs, ins, ref, b_alg in (
+        ("rfft_16384x1024", RFFT(xrs[0]), specs, xrs, full, xr.nbytes + 16384 * 513 * 8),
+        ("irfft_16384x1024", IRFFT(specs[0]), backs, specs, xr, xr.nbytes + 16384 * 513 * 8),
+        ("aprfft_16384x1024", APRFFT(xrs[0]), hs, xrs, harm, xr.nbytes + 16384 * 512 * 8),
+        ("iaprfft_16384x1024", IAPRFFT(hs[0]), backs, hs, xr, xr.nbytes + 16384 * 512 * 8),
+    ):
+        cc = comp.compile(dev)
+        us = timed(lambda o, i: cc(None, o, i), list(zip(outs, ins))) * 1e3
+        res[label] = entry(us, b_alg, rel(outs[0].cpu().numpy(), ref), cc.launches)
+    cpu = None
+    if not args.no_cpu_baseline:
+        # the oracle's FFT of the windowed frames (reikna's composition on the CPU),
+        # a bounded sample of frames scaled to the whole signal
+        from oracle import oracle
+
+        sample = 2048
+        fr = (sig[numpy.arange(sample)[:, None] * hop + numpy.arange(nfft)[None, :]] * win.astype(numpy.float32)).astype(
+            numpy.complex64)
+        plan = oracle.Plan(fr.shape, (1,))
+        times = []
+        t_end = time.perf_counter() + 6.0
+        while len(times) < 3 or (time.perf_counter() < t_end and len(times) < 30):
+            t0 = time.perf_counter()
+            numpy.abs(plan(fr, threads=os.cpu_count())[:, : nfft // 2 + 1])
+            times.append(time.perf_counter() - t0)
+        t = statistics.median(times[1:]) * nfr / sample
+        cpu = {"value": res["spectrogram"]["bytes_algorithmic"] / t / 1e9, "unit": "GB/s", "cores": os.cpu_count(),
+               "kind": "port", "sample": f"{sample} of {nfr} frames (window, complex64 FFT, magnitude, crop), scaled",
+               "ms_per_step": t * 1e3}
+    head = res["spectrogram_transposed"]
+    line = {
+        "metric": METRIC,
+        "value": head["gbs"],
+        "unit": "GB/s",
+        "n_gpus": 1,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": head["us"] / 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "next_rows_spectrogram_2^22_fftshift_transpose_4096^2_real_16384x1024",
+                   "l2": "two buffer sets alternate", "peak_gbs": peak, "peak_kind": peak_kind},
+        "results": res,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -805,10 +948,11 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["own", "reference"], default="own")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["fft3d", "serve", "precision", "batch"], default="fft3d",
+    ap.add_argument("--workload", choices=["fft3d", "serve", "precision", "batch", "next"], default="fft3d",
                     help="fft3d: the headline 256^3 transform; serve: the request stream; "
                     "precision: FP32 against the tensor-core split mode on 16384 x 1024; "
-                    "batch: the mixed-size batch in every batching mode")
+                    "batch: the mixed-size batch in every batching mode; next: spectrogram, FFTShift, "
+                    "Transpose and the real transforms")
     ap.add_argument("--requests", type=int, default=1000, help="serve: requests in the stream")
     ap.add_argument("--streams", type=int, default=4, help="serve: compute streams of the server")
     ap.add_argument("--load", type=float, default=0.7, help="serve: Poisson rate / served burst rate")
@@ -828,6 +972,8 @@ def main(argv=None) -> int:
         return run_precision(args, rank, world, local_rank)
     if args.workload == "batch":
         return run_batch(args, rank, world, local_rank)
+    if args.workload == "next":
+        return run_next(args, rank, world, local_rank)
     return run_own(args, rank, world, local_rank)
 
 

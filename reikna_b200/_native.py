@@ -44,6 +44,7 @@ FLAG_PAIR = 32
 FLAG_REAL_POST = 64
 FLAG_REAL_PRE = 128
 FLAG_ANTIPERIODIC = 256
+FLAG_NO_HALF = 512
 
 EXPORTED = (
     "rk_edge_init",

@@ -172,7 +172,25 @@ __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, 
     if (la.ok && a < s.ax_len) {
         int64_t u = a + s.ax_shift;
         if (u >= s.ax_len) u -= s.ax_len;
-        if (u < s.ax_bound) {
+        if ((s.flags & SF_RPAIR) && u < s.ax_bound) {
+            // a real signal read as sample pairs (x[2u], x[2u+1]); a window covers the
+            // sample index 2u / 2u + 1
+            const int64_t off = la.base + 2 * u * s.ax_stride;
+            T x0, x1;
+            if (s.fmt == RK_FMT_F64) {
+                x0 = (T)reinterpret_cast<const double*>(s.ptr)[off];
+                x1 = (T)reinterpret_cast<const double*>(s.ptr)[off + s.ax_stride];
+            } else {
+                x0 = (T)reinterpret_cast<const float*>(s.ptr)[off];
+                x1 = (T)reinterpret_cast<const float*>(s.ptr)[off + s.ax_stride];
+            }
+            if (s.flags & SF_WINDOW) {
+                const T* wt = reinterpret_cast<const T*>(s.win);
+                x0 *= wt ? (2 * u < s.win_len ? wt[2 * u] : T(1)) : hann<T>(2 * u, s.win_len);
+                x1 *= wt ? (2 * u + 1 < s.win_len ? wt[2 * u + 1] : T(1)) : hann<T>(2 * u + 1, s.win_len);
+            }
+            v = cmk<V>(x0, x1);
+        } else if (u < s.ax_bound) {
             const int64_t off = la.base + u * s.ax_stride;
             switch (s.fmt) {
                 case RK_FMT_C64: {
@@ -326,15 +344,100 @@ __device__ __forceinline__ cplx<T> edge_value(const Side& s, cplx<T> v) {
     return v;
 }
 
-// y A + conj(ym) B with A = h (1 - i w), B = h (1 + i w): the step between a real
-// signal's spectrum and the half-length complex spectrum of its sample pairs
+// The Nyquist bin X[L] of a real-spectrum store at element offset off: the side's
+// scale, then the complex value or, for a real output, |X|^post_param (SF_NORM) or
+// its real part.
 template <typename T>
-__device__ __forceinline__ cplx<T> real_mix(cplx<T> y, cplx<T> ym, cplx<T> w, T h) {
+__device__ __forceinline__ void store_nyquist(const Side& s, int64_t off, cplx<T> x) {
     using V = cplx<T>;
-    const V a = cmk<V>(h * (T(1) + w.y), -h * w.x);
-    const V b = cmk<V>(h * (T(1) - w.y), h * w.x);
-    const V x = cmul(y, a), z = cmul(cconj(ym), b);
-    return cmk<V>(x.x + z.x, x.y + z.y);
+    if (s.flags & SF_SCALE) x = cmul(x, cmk<V>((T)s.scale_re, (T)s.scale_im));
+    if (s.fmt == RK_FMT_C64 || s.fmt == RK_FMT_C128) {
+        reinterpret_cast<V*>(s.ptr)[off] = x;
+        return;
+    }
+    T r = x.x;
+    if (s.flags & SF_NORM) {
+        r = x.x * x.x + x.y * x.y;
+        if (s.post_param == 1.0)
+            r = sqrt(r);
+        else if (s.post_param != 2.0)
+            r = pow(r, (T)(s.post_param * 0.5));
+    }
+    reinterpret_cast<T*>(s.ptr)[off] = r;
+}
+
+// Bins of the pairwise real-signal step owned by thread tb of a line: slot q < RT/2
+// holds bin k_q = tb + TPL q (every k_q < L/2), slot RT/2 + q its mirror
+// L - k_q - rodd; without rodd the mirror of bin 0 is bin L (kept apart), so slot
+// RT/2 of thread 0 holds the self-mirrored bin L/2 instead.
+template <int L, int RT, int TPL>
+__device__ __forceinline__ int pair_pos(int tb, int i, int rodd) {
+    if (i < RT / 2) return tb + TPL * i;
+    const int k = tb + TPL * (i - RT / 2);
+    return (!rodd && k == 0) ? L / 2 : L - k - rodd;
+}
+
+// The step y[k] A_k + conj(y[m]) B_k for bin k and its mirror m at once: with
+// P = y[k], Q = conj(y[m]), S = h (P + Q) and D = -i h w_k (P - Q), bin k gets S + D
+// and bin m gets conj(S - D) (A_m = conj(A_k), B_m = conj(B_k) since w_m = -conj(w_k))
+template <typename T>
+__device__ __forceinline__ void real_pair(cplx<T> y, cplx<T> ym, cplx<T> w, T h, cplx<T>& ok, cplx<T>& om) {
+    using V = cplx<T>;
+    const V q = cconj(ym);
+    const V s = cmk<V>(h * (y.x + q.x), h * (y.y + q.y));
+    const V d = cmul(cmk<V>(y.x - q.x, y.y - q.y), cmk<V>(h * w.y, -h * w.x));
+    ok = cmk<V>(s.x + d.x, s.y + d.y);
+    om = cmk<V>(s.x - d.x, d.y - s.y);
+}
+
+// Forward step after the FFT: v[] (pair_pos order) from the half-length spectrum Z
+// read through zat(k); returns the Nyquist bin X[L] for thread 0 without rodd.
+template <typename T, int L, int RT, int TPL, class ZAt>
+__device__ __forceinline__ cplx<T> real_pairs_out(const PassParams& p, int tb, ZAt zat, cplx<T>* v) {
+    using V = cplx<T>;
+    const V* wk = reinterpret_cast<const V*>(p.rmix);
+    const T h = (T)p.rh;
+#pragma unroll
+    for (int q = 0; q < RT / 2; ++q) {
+        const int k = tb + TPL * q;
+        real_pair<T>(zat(k), zat((L - k - p.rodd) & (L - 1)), __ldg(wk + k), h, v[q], v[RT / 2 + q]);
+    }
+    V nyq = cmk<V>(T(0), T(0));
+    if (!p.rodd && tb == 0) {
+        nyq = v[RT / 2];
+        V unused;
+        const V zh = zat(L / 2);
+        real_pair<T>(zh, zh, __ldg(wk + L / 2), h, v[RT / 2], unused);
+    }
+    return nyq;
+}
+
+// Inverse step before the FFT, in place on v[] (pair_pos order: the raw bins y);
+// yl is bin L of the input row (the mirror of bin 0 without rodd).
+template <typename T, int L, int RT, int TPL>
+__device__ __forceinline__ void real_pairs_in(const PassParams& p, int tb, cplx<T> yl, cplx<T>* v) {
+    using V = cplx<T>;
+    const V* wk = reinterpret_cast<const V*>(p.rmix);
+    const T h = (T)p.rh;
+    const bool special = !p.rodd && tb == 0;
+    const V yh = v[RT / 2];  // bin L/2 in thread 0's slot RT/2 when special
+#pragma unroll
+    for (int q = 0; q < RT / 2; ++q) {
+        const int k = tb + TPL * q;
+        V y = v[q], ym = v[RT / 2 + q];
+        if (q == 0 && special) {
+            ym = yl;
+            if (p.rnyq) {
+                y.y = T(0);
+                ym.y = T(0);
+            }
+        }
+        real_pair<T>(y, ym, __ldg(wk + k), h, v[q], v[RT / 2 + q]);
+    }
+    if (special) {
+        V unused;
+        real_pair<T>(yh, yh, __ldg(wk + L / 2), h, v[RT / 2], unused);
+    }
 }
 
 template <typename T, int N, class PosF>
@@ -395,16 +498,35 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
         }
     } else if (f & SF_FASTR) {
         // real input of the pass precision (e.g. windowed signal frames): one line
-        // pointer, 32-bit offsets, the window from the plan's table
+        // pointer, 32-bit offsets, the window from the plan's table; SF_RPAIR reads the
+        // samples 2a and 2a + 1 as one element (one vector load on a contiguous,
+        // aligned line)
         const T* lp = reinterpret_cast<const T*>(s.ptr) + la.base;
         const T* wt = (f & SF_WINDOW) ? reinterpret_cast<const T*>(s.win) : nullptr;
         const int st = (int)s.ax_stride;
+        if (f & SF_RPAIR) {
+            // the pair vector load needs the line's address aligned to the pair type
+            const bool vec = st == 1 && (reinterpret_cast<uintptr_t>(lp) % sizeof(V)) == 0;
 #pragma unroll
-        for (int i = 0; i < N; ++i) {
-            const int a = pos(i);
-            T x = la.ok ? lp[a * st] : T(0);
-            if (wt) x *= __ldg(wt + a);
-            v[i] = cmk<V>(x, T(0));
+            for (int i = 0; i < N; ++i) {
+                const int a = pos(i);
+                V x = cmk<V>(T(0), T(0));
+                if (la.ok) x = vec ? reinterpret_cast<const V*>(lp)[a] : cmk<V>(lp[2 * a * st], lp[(2 * a + 1) * st]);
+                if (wt) {
+                    const V w = __ldg(reinterpret_cast<const V*>(wt) + a);
+                    x.x *= w.x;
+                    x.y *= w.y;
+                }
+                v[i] = x;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int a = pos(i);
+                T x = la.ok ? lp[a * st] : T(0);
+                if (wt) x *= __ldg(wt + a);
+                v[i] = cmk<V>(x, T(0));
+            }
         }
         if (f & SF_SCALE) scale_block<T, N>(s, v);
         if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
@@ -609,37 +731,26 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
     V v[RT];
     {
         const LineAddr la = line_addr(p.ld, line, p.C, p.I, lok);
-        load_block<T, RT>(p.ld, la, [&](int i) { return E::in_pos(tb, i / R0, i % R0); }, v);
         if constexpr (VAR == 4) {
             // half-length spectrum of a real signal from its bins y (the inverse real
-            // transforms; y arrives conjugated, as the inverse FFT's first load):
-            // y[k] A_k + conj(y[mirror k]) B_k; with rnyq the mirror of bin 0 is bin L
-            // of the input row, and bins 0 and L lose their imaginary parts
+            // transforms; y arrives conjugated, as the inverse FFT's first load), pair
+            // by pair; with rnyq the mirror of bin 0 is bin L of the input row, and
+            // bins 0 and L lose their imaginary parts
             static_assert(MODE == MODE_POS, "the real-signal step needs whole lines");
+            load_block<T, RT>(p.ld, la, [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
             V yl = cmk<V>(T(0), T(0));
             if (p.rnyq && la.ok) yl = edge_value<T>(p.ld, reinterpret_cast<const V*>(p.ld.ptr)[la.base + (int64_t)L * p.ld.ax_stride]);
+            real_pairs_in<T, L, RT, TPL>(p, tb, yl, v);
+#pragma unroll
+            for (int i = 0; i < RT; ++i) sm[E::sidx(ln, pair_pos<L, RT, TPL>(tb, i, p.rodd))] = v[i];
+            __syncthreads();
 #pragma unroll
             for (int z = 0; z < RT / R0; ++z)
 #pragma unroll
-                for (int m = 0; m < R0; ++m) sm[E::sidx(ln, E::in_pos(tb, z, m))] = v[z * R0 + m];
+                for (int m = 0; m < R0; ++m) v[z * R0 + m] = sm[E::sidx(ln, E::in_pos(tb, z, m))];
             __syncthreads();
-            const V* wk = reinterpret_cast<const V*>(p.rmix);
-            const T h = (T)p.rh;
-#pragma unroll
-            for (int z = 0; z < RT / R0; ++z)
-#pragma unroll
-                for (int m = 0; m < R0; ++m) {
-                    const int k = E::in_pos(tb, z, m);
-                    V yk = v[z * R0 + m];
-                    V ym = sm[E::sidx(ln, (L - k - p.rodd) & (L - 1))];
-                    if (p.rnyq && k == 0) {
-                        ym = yl;
-                        yk.y = T(0);
-                        ym.y = T(0);
-                    }
-                    v[z * R0 + m] = real_mix<T>(yk, ym, __ldg(wk + k), h);
-                }
-            __syncthreads();
+        } else {
+            load_block<T, RT>(p.ld, la, [&](int i) { return E::in_pos(tb, i / R0, i % R0); }, v);
         }
     }
     E::run(v, sm, ln, tb, tw);
@@ -673,24 +784,10 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
 #pragma unroll
             for (int m = 0; m < RL; ++m) sm[E::sidx(ln, E::out_pos(tb, z, m))] = v[z * RL + m];
         __syncthreads();
-        const V* wk = reinterpret_cast<const V*>(p.rmix);
-        const T h = (T)p.rh;
-#pragma unroll
-        for (int z = 0; z < RT / RL; ++z)
-#pragma unroll
-            for (int m = 0; m < RL; ++m) {
-                const int k = E::out_pos(tb, z, m);
-                v[z * RL + m] = real_mix<T>(sm[E::sidx(ln, k)], sm[E::sidx(ln, (L - k - p.rodd) & (L - 1))],
-                                            __ldg(wk + k), h);
-            }
+        const V nyq = real_pairs_out<T, L, RT, TPL>(p, tb, [&](int k) { return sm[E::sidx(ln, k)]; }, v);
         const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
-        if (tb == 0 && la.ok && p.rnyq) {
-            const V z0 = sm[E::sidx(ln, 0)];
-            V xl = cmk<V>(z0.x - z0.y, T(0));
-            if (p.st.flags & SF_SCALE) xl = cmul(xl, cmk<V>((T)p.st.scale_re, (T)p.st.scale_im));
-            reinterpret_cast<V*>(p.st.ptr)[la.base + (int64_t)L * p.st.ax_stride] = xl;
-        }
-        store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
+        if (tb == 0 && la.ok && p.rnyq) store_nyquist<T>(p.st, la.base + (int64_t)L * p.st.ax_stride, nyq);
+        store_block<T, RT>(p.st, p, la, [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
     } else if constexpr (VAR == 2) {
         static_assert(MODE == MODE_POS, "transposed store needs position mode");
 #pragma unroll

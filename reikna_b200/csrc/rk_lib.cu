@@ -192,11 +192,12 @@ __global__ void k_gen_rodd(int64_t L, float2* f, double2* d) {
     if (d) d[k] = make_double2(c, s);
 }
 
-// von Hann window 0.5 (1 - cos(2 pi u / (w - 1))), u < w, in FP64, rounded once
-__global__ void k_gen_window(int32_t w, float* f, double* d) {
-    const int32_t u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= w) return;
-    const double v = w > 1 ? 0.5 * (1.0 - cospi(2.0 * (double)u / (double)(w - 1))) : 1.0;
+// von Hann window 0.5 (1 - cos(2 pi u / (w - 1))) for u < w and 1 beyond, u < n, in
+// FP64, rounded once
+__global__ void k_gen_window(int64_t n, int32_t w, float* f, double* d) {
+    const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    const double v = u >= w ? 1.0 : (w > 1 ? 0.5 * (1.0 - cospi(2.0 * (double)u / (double)(w - 1))) : 1.0);
     if (f) f[u] = (float)v;
     if (d) d[u] = v;
 }
@@ -275,6 +276,28 @@ static int64_t prod_range(const int64_t* s, int a, int b) {
     return p;
 }
 
+// A transform of the last axis only, of a real input of the plan's precision, whose
+// output keeps at most the bins 0 .. N/2 contiguously (a spectrogram, or
+// real_to_complex + crop_frequencies), N/2 a power of two one pass covers: the
+// half-length route applies.  Any conjugation or scale of the input is folded into
+// the output per call (the input is real, the transform linear).
+static bool half_eligible(const rk_fft_desc& d, int dbl) {
+    if (d.flags & (RK_FLAG_NO_HALF | RK_FLAG_REAL_POST | RK_FLAG_REAL_PRE)) return false;
+    const int nd = d.ndim, ax = nd - 1;
+    if (d.naxes != 1 || d.axes[0] != ax) return false;
+    const int64_t n = d.shape[ax];
+    if (n % 2) return false;
+    const int64_t L = n / 2;
+    if (!is_pow2(L) || L < 8 || L > (dbl ? 4096 : 8192)) return false;
+    const rk_edge& in = d.input;
+    const rk_edge& out = d.output;
+    const int rfmt = dbl ? RK_FMT_F64 : RK_FMT_F32, cfmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
+    if (in.format != rfmt || in.shape[ax] != n || in.shift[ax] != 0) return false;
+    if (in.window != RK_WIN_NONE && in.window_axis != ax) return false;
+    if (out.shift[ax] != 0 || out.shape[ax] > L + 1 || out.strides[ax] != 1) return false;
+    return out.format == cfmt || (out.format == rfmt && out.post == RK_POST_NORM);
+}
+
 static int plan_passes(const rk_fft_desc& d, Planned& P) {
     const int dbl = d.dtype == RK_FMT_C128;
     std::vector<int> axes(d.axes, d.axes + d.naxes);
@@ -316,6 +339,25 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
         p.ld.cA = p.st.cA = 1;
         p.ld.jB = p.st.jB = 0;
         p.note = "copy";
+        P.passes.push_back(p);
+        return RK_OK;
+    }
+
+    if (half_eligible(d, dbl)) {
+        // a real signal along the last axis whose output keeps at most the bins
+        // 0 .. N/2: one pass of the half-length FFT over the sample pairs
+        // x[2u] + i x[2u+1], with the real-spectrum step in its store (the RFFT of
+        // examples/demo_specialized_fft.py:175-241, chosen by the planner)
+        const int ax = nd - 1;
+        PassSpec p;
+        p.L = (int)(d.shape[ax] / 2);
+        p.mode = MODE_POS;
+        p.var = 3;
+        p.axis = ax;
+        p.O = prod_range(d.shape, 0, ax);
+        p.ld.buf = SB_IN; p.ld.ax_len = p.L; p.ld.cA = 0; p.ld.jB = 1; p.ld.flags = SF_RPAIR;
+        p.st.buf = SB_OUT; p.st.ax_len = p.L; p.st.cA = 0; p.st.jB = 1;
+        p.note = "half";
         P.passes.push_back(p);
         return RK_OK;
     }
@@ -655,9 +697,16 @@ static void setup_tma(PassRec& r, int dbl, int nsm) {
     const Side& ld = p.ld;
     const Side& st = p.st;
     const int esz = dbl ? 16 : 8;
-    if (!(ld.flags & SF_FAST) || !(st.flags & SF_FAST) || ld.ax_shift != 0 || p.C != 1) return;
+    // sides: the lean block paths; the antiperiodic forward transform's load table
+    // (variant 3) and inverse transform's store table (variant 4) are applied by the
+    // TMA kernel and store_block; the inverse real step reads whole rows of L bins
+    const bool ld_ok = (ld.flags & SF_FAST) ||
+                       (r.var == 3 && (ld.flags & SF_FAST2) && !(ld.flags & ~(SF_FAST2 | SF_TAB | SF_SCALE)) &&
+                        ld.cA == 0 && ld.jB == 1 && ld.ax_len == r.L && ld.ax_bound == r.L);
+    const bool st_ok = (st.flags & SF_FAST) || (r.var == 4 && (st.flags & SF_FAST2));
+    if (!ld_ok || !st_ok || ld.ax_shift != 0 || p.C != 1 || (r.var == 4 && p.rnyq)) return;
     TmaInfo ti;
-    if (!tma_info(dbl, r.L, r.mode, &ti)) return;
+    if (!tma_info(dbl, r.L, r.mode, r.var, &ti)) return;
     const int64_t L = r.L, NL = ti.nl;
     for (int i = 0; i < ld.nd_o; ++i)
         if (ld.o_shift[i] != 0 || ld.o_bound[i] != ld.o_shape[i]) return;
@@ -715,11 +764,13 @@ static void mark_fastr(Side& s, int dbl, int64_t L, bool load) {
     if (s.flags & (SF_FAST | SF_FAST2)) return;
     const int fmt = dbl ? RK_FMT_F64 : RK_FMT_F32;
     if (s.fmt != fmt || s.cA != 0 || s.jB != 1 || s.ax_shift != 0 || s.ax_stride < 0 || s.ax_len != L) return;
-    if ((L - 1) * std::max<int64_t>(s.ax_stride, 1) >= (int64_t(1) << 31)) return;
+    const int64_t span = (s.flags & SF_RPAIR) ? 2 * L : L;  // samples along the axis
+    if ((span - 1) * std::max<int64_t>(s.ax_stride, 1) >= (int64_t(1) << 31)) return;
     const int32_t conj = SF_PRE_CONJ | SF_POST_CONJ | SF_SCALE;
     if (load) {
-        if (s.ax_bound != s.ax_len || (s.flags & ~(conj | SF_WINDOW))) return;
-        if ((s.flags & SF_WINDOW) && (!s.win || s.win_len < L)) return;  // the table covers every position
+        if (s.ax_bound != s.ax_len || (s.flags & ~(conj | SF_WINDOW | SF_RPAIR))) return;
+        // the window table covers every position (pair-read sides: padded to 2L)
+        if ((s.flags & SF_WINDOW) && (!s.win || (!(s.flags & SF_RPAIR) && s.win_len < L))) return;
     } else {
         if (s.ax_bound > s.ax_len || (s.flags & ~(conj | SF_NORM))) return;
     }
@@ -1046,11 +1097,14 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         if (!r.ld_edge) pp.ld.ptr = bufs[ps.ld.buf];
         if (!r.st_edge) pp.st.ptr = bufs[ps.st.buf];
         if ((pp.ld.flags & SF_WINDOW) && pp.ld.win_len > 0) {
+            // a pair-read side indexes the samples 2u and 2u + 1 of every position u < L
+            const int64_t n = (pp.ld.flags & SF_RPAIR) ? std::max<int64_t>(pp.ld.win_len, 2 * (int64_t)ps.L)
+                                                       : (int64_t)pp.ld.win_len;
             void* wt = nullptr;
-            const int wrc = alloc((int64_t)pp.ld.win_len * (dbl ? 8 : 4), &wt);
+            const int wrc = alloc(n * (dbl ? 8 : 4), &wt);
             if (wrc) return fail(wrc);
-            k_gen_window<<<(pp.ld.win_len + 255) / 256, 256>>>(pp.ld.win_len, dbl ? nullptr : (float*)wt,
-                                                               dbl ? (double*)wt : nullptr);
+            k_gen_window<<<(unsigned)((n + 255) / 256), 256>>>(n, pp.ld.win_len, dbl ? nullptr : (float*)wt,
+                                                              dbl ? (double*)wt : nullptr);
             CK(cudaGetLastError());
             pp.ld.win = wt;
         }
@@ -1059,8 +1113,12 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             mark_fastr(pp.st, dbl, ps.L, false);
         }
         if (ps.var == 3 || ps.var == 4) {
-            const int cfmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
-            if (pp.st.fmt != cfmt || pp.ld.fmt != cfmt) {
+            const int cfmt = dbl ? RK_FMT_C128 : RK_FMT_C64, rfmt = dbl ? RK_FMT_F64 : RK_FMT_F32;
+            const bool edges_ok = (pp.ld.flags & SF_RPAIR)
+                                      ? (pp.ld.fmt == rfmt &&
+                                         (pp.st.fmt == cfmt || (pp.st.fmt == rfmt && (pp.st.flags & SF_NORM))))
+                                      : (pp.st.fmt == cfmt && pp.ld.fmt == cfmt);
+            if (!edges_ok) {
                 set_error("a one-pass real transform needs complex edges of the transform's precision");
                 return fail(RK_ERR_UNSUPPORTED);
             }
@@ -1151,7 +1209,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             }
             r.nblocks = (pp.nlines + li.nl - 1) / li.nl;
             r.li = li;
-            if (!(desc->flags & RK_FLAG_NO_TMA) && ps.var == 0) setup_tma(r, dbl, nsm);
+            if (!(desc->flags & RK_FLAG_NO_TMA) && (ps.var == 0 || ps.var == 3 || ps.var == 4)) setup_tma(r, dbl, nsm);
             if ((desc->flags & RK_FLAG_SPLIT_TC) && tc_eligible(r)) {
                 r.use_tc = true;
                 r.use_tma = false;
@@ -1383,6 +1441,28 @@ int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs
             if (i == np - 1) p.st.flags ^= SF_POST_CONJ;
         }
         if (r.st_edge && d.output.conj) p.st.flags ^= SF_POST_CONJ;
+        if (p.ld.flags & SF_RPAIR) {
+            // the half-length route reads a real signal as sample pairs: a multiplier c
+            // of the input (conjugated by the input's conjugations) multiplies the
+            // transform, so it moves to the store, conjugated once more by the store's
+            // conjugation (the store conjugates X before scaling)
+            double cr = 1.0, ci = 0.0;
+            if (p.ld.flags & SF_SCALE) { cr = p.ld.scale_re; ci = p.ld.scale_im; }
+            const bool ld_conj = ((p.ld.flags & SF_PRE_CONJ) != 0) != ((p.ld.flags & SF_POST_CONJ) != 0);
+            const bool st_conj = ((p.st.flags & SF_PRE_CONJ) != 0) != ((p.st.flags & SF_POST_CONJ) != 0);
+            if (ld_conj != st_conj) ci = -ci;
+            p.ld.flags &= ~(SF_SCALE | SF_PRE_CONJ | SF_POST_CONJ);
+            double sr = 1.0, si = 0.0;
+            if (p.st.flags & SF_SCALE) { sr = p.st.scale_re; si = p.st.scale_im; }
+            const double nr = sr * cr - si * ci, ni = sr * ci + si * cr;
+            if (nr != 1.0 || ni != 0.0) {
+                p.st.flags |= SF_SCALE;
+                p.st.scale_re = nr;
+                p.st.scale_im = ni;
+            } else {
+                p.st.flags &= ~SF_SCALE;
+            }
+        }
         out.push_back(p);
         if (tma_ok) tma_ok->push_back(tma ? 1 : 0);
     }

@@ -25,6 +25,7 @@ enum SideFlags : int32_t {
     SF_FAST = 256,      // pass-dtype side, a = j, no axis padding, power-of-two axis
     SF_FAST2 = 512,     // pass-dtype side, a = c cA + j jB, no remap, 32-bit offsets
     SF_FASTR = 1024,    // real side of the pass precision, a = j, no remap, 32-bit offsets
+    SF_RPAIR = 2048,    // real load side read as sample pairs: element u = x[2u] + i x[2u+1]
 };
 
 // Addressing of one buffer in a pass.  A line l in [0, O*C*I) decomposes as

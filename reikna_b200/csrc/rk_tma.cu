@@ -16,137 +16,16 @@
 
 #include <mutex>
 
-#include "rk_async.cuh"
-#include "rk_internal.h"
-#include "rk_kernels.cuh"
+#include "rk_tma.cuh"
 
 namespace rk {
 
-template <typename T, int L, int MODE> struct TmaCfg {
-    using Cfg = LineCfg<T, L, MODE>;
-    static constexpr int NL = Cfg::NL, NT = Cfg::NT, ESZ = Cfg::ESZ;
-    static constexpr int TILE = NL * L;                                           // elements copied
-    static constexpr int BUF = MODE == MODE_POS ? NL * Cfg::LS : NL * L;          // elements per buffer
-    static constexpr size_t SMEM = 2 * (size_t)BUF * ESZ + 64;                     // + 2 mbarriers
-};
-
-template <typename T, int L, int MODE>
-__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line_tma(const __grid_constant__ PassParams p) {
-    using V = cplx<T>;
-    using E = Engine<T, L, MODE>;
-    using C = TmaCfg<T, L, MODE>;
-    constexpr int RT = E::RT, TPL = E::TPL, NL = E::NL, R0 = E::R0, RL = E::RL;
-    extern __shared__ __align__(128) unsigned char rk_smem[];
-    V* buf0 = reinterpret_cast<V*>(rk_smem);
-    V* buf1 = buf0 + C::BUF;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(buf1 + C::BUF);
-    const V* tw = reinterpret_cast<const V*>(p.tw);
-    const int tid = threadIdx.x;
-    const int ln = MODE == MODE_POS ? tid / TPL : tid % NL;
-    const int tb = MODE == MODE_POS ? tid % TPL : tid / NL;
-
-    auto issue = [&](int64_t t, int b) {
-        V* dst = b ? buf1 : buf0;
-        uint64_t* bar = bars + b;
-        if (p.tma_mode == TMA_BULK) {
-            const int64_t first = t * NL;
-            const int64_t nl = (p.nlines - first) < NL ? (p.nlines - first) : NL;
-            const uint32_t bytes = (uint32_t)(nl * L * C::ESZ);
-            mbar_arrive_expect_tx(bar, bytes);
-            const V* src = reinterpret_cast<const V*>(p.ld.ptr) + p.ld.offset + t * p.tile_stride;
-            bulk_g2s(dst, src, bytes, bar);
-        } else {
-            const int64_t first = t * NL;
-            const int64_t o = first / p.I, i = first % p.I;
-            const int rows = L / p.tma_boxes;
-            mbar_arrive_expect_tx(bar, (uint32_t)(C::TILE * C::ESZ));
-            const int xs = sizeof(T) == 8 ? 2 : 1;  // complex128 maps as pairs of doubles
-            for (int k = 0; k < p.tma_boxes; ++k)
-                tma_g2s_3d(dst + (size_t)k * rows * NL, &p.tmap, (int)i * xs, k * rows, (int)o, bar);
-        }
-    };
-
-    if (tid == 0) {
-        mbar_init(bars + 0, 1);
-        mbar_init(bars + 1, 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    const int64_t stride = gridDim.x;
-    int64_t t = blockIdx.x;
-    if (tid == 0) {
-        if (t < p.ntiles) issue(t, 0);
-        if (t + stride < p.ntiles) issue(t + stride, 1);
-    }
-    uint32_t phase0 = 0, phase1 = 0;
-    for (int k = 0; t < p.ntiles; t += stride, ++k) {
-        const int b = k & 1;
-        V* buf = b ? buf1 : buf0;
-        const bool ok = mbar_wait(bars + b, b ? phase1 : phase0, p.status);
-        if (b) phase1 ^= 1; else phase0 ^= 1;
-        if (!ok) {
-            // the status word records the timeout; before leaving, give the copy into
-            // the other buffer (if one was issued) a bounded chance to land
-            if (t + stride < p.ntiles) mbar_wait(bars + (b ^ 1), b ? phase0 : phase1, nullptr);
-            break;
-        }
-        V v[RT];
-#pragma unroll
-        for (int z = 0; z < RT / R0; ++z)
-#pragma unroll
-            for (int m = 0; m < R0; ++m) {
-                const int pos = E::in_pos(tb, z, m);
-                v[z * R0 + m] = MODE == MODE_POS ? buf[ln * L + pos] : buf[pos * NL + ln];
-            }
-        if (p.ld.flags & SF_SCALE) {
-            const V c = cmk<V>((T)p.ld.scale_re, (T)p.ld.scale_im);
-#pragma unroll
-            for (int i = 0; i < RT; ++i) v[i] = cmul(v[i], c);
-        }
-        if (((p.ld.flags & SF_PRE_CONJ) != 0) != ((p.ld.flags & SF_POST_CONJ) != 0)) {
-#pragma unroll
-            for (int i = 0; i < RT; ++i) v[i].y = -v[i].y;
-        }
-        __syncthreads();  // the tile is in registers: the buffer becomes the exchange area
-        E::run(v, buf, ln, tb, tw);
-        if constexpr (E::NS == 1) __syncthreads();
-        if (tid == 0 && t + 2 * stride < p.ntiles) {
-            fence_proxy_async_smem();
-            issue(t + 2 * stride, b);
-        }
-        const int64_t line = t * NL + ln;
-        const LineAddr la = line_addr(p.st, line, p.C, p.I, line < p.nlines);
-        store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
-    }
-}
-
-template <typename T, int L, int MODE> struct TmaLauncher {
-    using C = TmaCfg<T, L, MODE>;
-    static cudaError_t launch(const PassParams& p, int64_t nblocks, cudaStream_t st) {
-        static bool attr_done = false;
-        if (!attr_done) {
-            cudaError_t e =
-                cudaFuncSetAttribute(k_line_tma<T, L, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-            if (e != cudaSuccess) return e;
-            attr_done = true;
-        }
-        if (nblocks <= 0) return cudaSuccess;
-        k_line_tma<T, L, MODE><<<(unsigned)nblocks, C::NT, C::SMEM, st>>>(p);
-        return cudaGetLastError();
-    }
-    static int per_sm() {
-        int n = 0;
-        cudaFuncSetAttribute(k_line_tma<T, L, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_line_tma<T, L, MODE>, C::NT, C::SMEM);
-        return n;
-    }
-    static TmaInfo info() { return TmaInfo{&launch, &per_sm, C::NT, C::NL, C::SMEM}; }
-};
-
 #define RK_TI(TY, LL, MODE) \
-    if (L == LL && mode == MODE) { *out = TmaLauncher<TY, LL, MODE>::info(); return true; }
+    if (L == LL && mode == MODE) { *out = TmaLauncher<TY, LL, MODE, 0>::info(); return true; }
 
-bool tma_info(int dbl, int L, int mode, TmaInfo* out) {
+bool tma_info(int dbl, int L, int mode, int var, TmaInfo* out) {
+    if (var == 3 || var == 4) return tma_info_real(dbl, L, mode, var, out);
+    if (var != 0) return false;
     if (!dbl) {
         RK_TI(float, 64, MODE_POS)
         RK_TI(float, 128, MODE_POS)

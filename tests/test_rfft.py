@@ -261,3 +261,71 @@ def test_real_plans_run_in_their_direction_only():
             plan.execute([b.data_ptr()], [a.data_ptr()], inverse=wrong, stream=0)
         plan.execute([b.data_ptr()], [a.data_ptr()], inverse=1 - wrong, stream=0)
     torch.cuda.synchronize()
+
+
+def _r2c_crop_fft(meta_real, cdt, flags_note=None):
+    from reikna_b200 import transformations as tr
+    from reikna_b200.core import ArrayMetadata
+    from reikna_b200.fft import FFT
+
+    fft = FFT(ArrayMetadata(tuple(meta_real.shape), cdt), axes=(len(meta_real.shape) - 1,))
+    scale = tr.mul_param(fft.parameter.input, cdt)
+    fft.parameter.input.connect(scale, scale.parameter.output, scaled=scale.parameter.input, k=scale.parameter.param)
+    r2c = tr.real_to_complex(meta_real)
+    fft.parameter.scaled.connect(r2c, r2c.parameter.output, real=r2c.parameter.input)
+    crop = tr.crop_frequencies(fft.parameter.output)
+    fft.parameter.output.connect(crop, crop.parameter.input, half=crop.parameter.output)
+    return fft
+
+
+def test_real_input_with_cropped_output_plans_the_half_route():
+    from reikna_b200.core import ArrayMetadata
+
+    fft = _r2c_crop_fft(ArrayMetadata((37, 1024), numpy.float32), numpy.complex64)
+    p = fft.describe()["passes"]
+    assert len(p) == 1 and p[0]["note"] == "half" and p[0]["L"] == 512 and p[0]["var"] == 3
+    # an odd length, or an output keeping the negative frequencies, keeps the full transform
+    assert _r2c_crop_fft(ArrayMetadata((37, 1000), numpy.float32), numpy.complex64).describe()["passes"][0]["note"] != "half"
+    from reikna_b200 import transformations as tr
+    from reikna_b200.fft import FFT
+
+    full = FFT(ArrayMetadata((37, 1024), numpy.complex64), axes=(1,))
+    r2c = tr.real_to_complex(ArrayMetadata((37, 1024), numpy.float32))
+    full.parameter.input.connect(r2c, r2c.parameter.output, real=r2c.parameter.input)
+    assert full.describe()["passes"][0]["note"] != "half"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows,n,dtype", [(37, 1024, numpy.float32), (5, 8192, numpy.float64), (64, 16, numpy.float32),
+                                          (3, 16384, numpy.float32)])
+@pytest.mark.parametrize("inverse", [0, 1])
+@pytest.mark.parametrize("offset", [0, 1])
+def test_half_route_for_real_input(rows, n, dtype, inverse, offset):
+    """A real input transformed along the last axis and cropped to n/2 + 1 bins runs as
+    the half-length transform of its sample pairs; a complex runtime scale of the input
+    and the inverse direction act through the store (the input is real).  offset 1
+    starts every row on an odd sample (no paired vector loads)."""
+    import torch
+
+    from reikna_b200.core import ArrayMetadata
+
+    cdt = numpy.complex64 if dtype == numpy.float32 else numpy.complex128
+    rng = numpy.random.default_rng(67)
+    x = rng.standard_normal((rows, n + offset)).astype(dtype)
+    t = torch.from_numpy(x).cuda()[:, offset:]
+    fft = _r2c_crop_fft(ArrayMetadata.from_arraylike(t), cdt)
+    assert fft.describe()["passes"][0]["note"] == "half"
+    out = torch.empty((rows, n // 2 + 1), dtype=torch.complex64 if cdt == numpy.complex64 else torch.complex128,
+                      device="cuda")
+    k = 0.75 - 1.5j
+    fft.compile()(None, out, t, k=k, inverse=inverse)
+    torch.cuda.synchronize()
+    xs = x[:, offset:].astype(numpy.float64) * k
+    ref = (numpy.fft.ifft if inverse else numpy.fft.fft)(xs, axis=1)[:, : n // 2 + 1]
+    assert rel_l2(out.cpu().numpy(), ref) < fft_bound(cdt, n)
+    # the same computation through the full-length route
+    full = torch.empty_like(out)
+    fft.compile(flags=2**9)(None, full, t, k=k, inverse=inverse)
+    torch.cuda.synchronize()
+    assert fft.compile(flags=2**9)._runner.plan.describe()["passes"][0]["note"] != "half"
+    assert rel_l2(full.cpu().numpy(), ref) < fft_bound(cdt, n)

@@ -17,8 +17,11 @@ def test_transposed_spectrogram_plans_a_lane_fastest_store():
 
     d = spectrogram(2**14, 256, 64, transposed=True).describe()
     assert len(d["passes"]) == 1 and d["passes"][0]["var"] == 2
+    # frame-major: the half-length transform of the windowed sample pairs with the
+    # real-spectrum step and the magnitude in its store
     d = spectrogram(2**14, 256, 64).describe()
-    assert d["passes"][0]["var"] == 0
+    p = d["passes"]
+    assert len(p) == 1 and p[0]["note"] == "half" and p[0]["var"] == 3 and p[0]["L"] == 128
 
 
 def test_transpose_2d_shape_and_errors():
