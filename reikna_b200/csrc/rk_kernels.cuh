@@ -773,11 +773,12 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
         __syncthreads();
         E::run(v, sm, ln, tb, tw);
     }
-    if constexpr (VAR == 3) {
+    if constexpr (VAR == 3 || VAR == 5) {
         // real-signal spectrum from the half-length spectrum Z of this line (the line
         // holds x[2n] + i x[2n+1]): X[k] = Z[k] A_k + conj(Z[mirror k]) B_k with the
         // plan's FP64-generated w_k in rmix; with rnyq the Nyquist bin
-        // X[L] = Re Z[0] - Im Z[0] is stored after the line's L positions
+        // X[L] = Re Z[0] - Im Z[0] is stored after the line's L positions.  Variant 5
+        // then stores lane-fastest through shared memory, as variant 2 does.
         static_assert(MODE == MODE_POS, "the real-spectrum step needs whole lines");
 #pragma unroll
         for (int z = 0; z < RT / RL; ++z)
@@ -787,7 +788,21 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
         const V nyq = real_pairs_out<T, L, RT, TPL>(p, tb, [&](int k) { return sm[E::sidx(ln, k)]; }, v);
         const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
         if (tb == 0 && la.ok && p.rnyq) store_nyquist<T>(p.st, la.base + (int64_t)L * p.st.ax_stride, nyq);
-        store_block<T, RT>(p.st, p, la, [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
+        if constexpr (VAR == 3) {
+            store_block<T, RT>(p.st, p, la, [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
+        } else {
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < RT; ++i) sm[E::sidx(ln, pair_pos<L, RT, TPL>(tb, i, p.rodd))] = v[i];
+            __syncthreads();
+            const int lane = tid % NL;
+            const int p0 = tid / NL;
+            const int64_t sline = block * NL + lane;
+            const LineAddr ls = line_addr(p.st, sline, p.C, p.I, sline < p.nlines);
+#pragma unroll
+            for (int q = 0; q < RT; ++q) v[q] = sm[E::sidx(lane, p0 + TPL * q)];
+            store_block<T, RT>(p.st, p, ls, [&](int q) { return p0 + TPL * q; }, v);
+        }
     } else if constexpr (VAR == 2) {
         static_assert(MODE == MODE_POS, "transposed store needs position mode");
 #pragma unroll

@@ -281,21 +281,26 @@ static int64_t prod_range(const int64_t* s, int a, int b) {
 // real_to_complex + crop_frequencies), N/2 a power of two one pass covers: the
 // half-length route applies.  Any conjugation or scale of the input is folded into
 // the output per call (the input is real, the transform linear).
-static bool half_eligible(const rk_fft_desc& d, int dbl) {
-    if (d.flags & (RK_FLAG_NO_HALF | RK_FLAG_REAL_POST | RK_FLAG_REAL_PRE)) return false;
+// Returns the line-pass variant: 3 (bins stored along the line), 5 (a transposed
+// output whose lines are adjacent in memory: bins stored lane-fastest), 0 = no.
+static int half_eligible(const rk_fft_desc& d, int dbl) {
+    if (d.flags & (RK_FLAG_NO_HALF | RK_FLAG_REAL_POST | RK_FLAG_REAL_PRE)) return 0;
     const int nd = d.ndim, ax = nd - 1;
-    if (d.naxes != 1 || d.axes[0] != ax) return false;
+    if (d.naxes != 1 || d.axes[0] != ax) return 0;
     const int64_t n = d.shape[ax];
-    if (n % 2) return false;
+    if (n % 2) return 0;
     const int64_t L = n / 2;
-    if (!is_pow2(L) || L < 8 || L > (dbl ? 4096 : 8192)) return false;
+    if (!is_pow2(L) || L < 8 || L > (dbl ? 4096 : 8192)) return 0;
     const rk_edge& in = d.input;
     const rk_edge& out = d.output;
     const int rfmt = dbl ? RK_FMT_F64 : RK_FMT_F32, cfmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
-    if (in.format != rfmt || in.shape[ax] != n || in.shift[ax] != 0) return false;
-    if (in.window != RK_WIN_NONE && in.window_axis != ax) return false;
-    if (out.shift[ax] != 0 || out.shape[ax] > L + 1 || out.strides[ax] != 1) return false;
-    return out.format == cfmt || (out.format == rfmt && out.post == RK_POST_NORM);
+    if (in.format != rfmt || in.shape[ax] != n || in.shift[ax] != 0) return 0;
+    if (in.window != RK_WIN_NONE && in.window_axis != ax) return 0;
+    if (out.shift[ax] != 0 || out.shape[ax] > L + 1) return 0;
+    if (!(out.format == cfmt || (out.format == rfmt && out.post == RK_POST_NORM))) return 0;
+    if (out.strides[ax] == 1) return 3;
+    if (ax > 0 && out.strides[ax - 1] == 1 && d.shape[ax - 1] > 1 && L <= lane_max(dbl)) return 5;
+    return 0;
 }
 
 static int plan_passes(const rk_fft_desc& d, Planned& P) {
@@ -343,7 +348,7 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
         return RK_OK;
     }
 
-    if (half_eligible(d, dbl)) {
+    if (const int hv = half_eligible(d, dbl)) {
         // a real signal along the last axis whose output keeps at most the bins
         // 0 .. N/2: one pass of the half-length FFT over the sample pairs
         // x[2u] + i x[2u+1], with the real-spectrum step in its store (the RFFT of
@@ -352,7 +357,7 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
         PassSpec p;
         p.L = (int)(d.shape[ax] / 2);
         p.mode = MODE_POS;
-        p.var = 3;
+        p.var = hv;
         p.axis = ax;
         p.O = prod_range(d.shape, 0, ax);
         p.ld.buf = SB_IN; p.ld.ax_len = p.L; p.ld.cA = 0; p.ld.jB = 1; p.ld.flags = SF_RPAIR;
@@ -1112,7 +1117,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             mark_fastr(pp.ld, dbl, ps.L, true);
             mark_fastr(pp.st, dbl, ps.L, false);
         }
-        if (ps.var == 3 || ps.var == 4) {
+        if (ps.var == 3 || ps.var == 4 || ps.var == 5) {
             const int cfmt = dbl ? RK_FMT_C128 : RK_FMT_C64, rfmt = dbl ? RK_FMT_F64 : RK_FMT_F32;
             const bool edges_ok = (pp.ld.flags & SF_RPAIR)
                                       ? (pp.ld.fmt == rfmt &&
@@ -1139,7 +1144,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             pp.rodd = ap ? 1 : 0;
             // forward: 2 (Z A + conj(Z') B) for the odd harmonics (the doubled half
             // period); inverse: one half of the forward's A, B (a quarter for them)
-            pp.rh = ps.var == 3 ? (ap ? 1.0 : 0.5) : (ap ? 0.25 : 0.5);
+            pp.rh = ps.var != 4 ? (ap ? 1.0 : 0.5) : (ap ? 0.25 : 0.5);
             pp.rnyq = ap ? 0 : (ps.var == 4 ? 1 : (desc->output.shape[ps.axis] > L ? 1 : 0));
             if (ap_tab) {
                 void* tt = nullptr;

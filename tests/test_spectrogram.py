@@ -15,7 +15,11 @@ def _reference(sig, nfft, hop):
 def test_transposed_spectrogram_plans_a_lane_fastest_store():
     from reikna_b200.spectrogram import spectrogram
 
+    # bins-by-frames: the same half-length pass, storing lane-fastest (variant 5); the
+    # full-length route stores lane-fastest with variant 2
     d = spectrogram(2**14, 256, 64, transposed=True).describe()
+    assert len(d["passes"]) == 1 and d["passes"][0]["var"] == 5 and d["passes"][0]["note"] == "half"
+    d = spectrogram(2**14, 256, 64, transposed=True).describe(flags=2**9)
     assert len(d["passes"]) == 1 and d["passes"][0]["var"] == 2
     # frame-major: the half-length transform of the windowed sample pairs with the
     # real-spectrum step and the magnitude in its store
@@ -35,9 +39,10 @@ def test_transpose_2d_shape_and_errors():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("length,nfft,hop", [(2**16, 1024, 256), (2**22, 1024, 256), (10000, 256, 100)])
+@pytest.mark.parametrize("length,nfft,hop", [(2**16, 1024, 256), (2**22, 1024, 256), (10000, 256, 100), (5000, 64, 16), (2**15, 2048, 512)])
 @pytest.mark.parametrize("transposed", [False, True])
-def test_spectrogram(length, nfft, hop, transposed):
+@pytest.mark.parametrize("flags", [0, 2**9])
+def test_spectrogram(length, nfft, hop, transposed, flags):
     import torch
 
     from reikna_b200.spectrogram import frames, spectrogram
@@ -52,7 +57,7 @@ def test_spectrogram(length, nfft, hop, transposed):
     nf = frames(length, nfft, hop)
     shape = (nfft // 2 + 1, nf) if transposed else (nf, nfft // 2 + 1)
     out = torch.empty(shape, dtype=torch.float32, device="cuda")
-    comp.compile()(None, out, torch.from_numpy(sig).cuda())
+    comp.compile(flags=flags)(None, out, torch.from_numpy(sig).cuda())
     torch.cuda.synchronize()
     ref = _reference(sig, nfft, hop)
     if transposed:
