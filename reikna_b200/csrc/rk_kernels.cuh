@@ -164,6 +164,17 @@ template <typename T> __device__ __forceinline__ T hann(int64_t u, int32_t w) {
     return T(0.5) * (T(1) - cospi(x));
 }
 
+// Square root for magnitudes (|z| = sqrt(re^2 + im^2), the norm post-operation of
+// order 1): the hardware's approximate single-precision square root (relative error
+// about 2^-23, below the transform's own rounding) for float, the correctly rounded
+// one for double.
+template <typename T> __device__ __forceinline__ T mag_sqrt(T x) { return sqrt(x); }
+template <> __device__ __forceinline__ float mag_sqrt<float>(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 template <typename T>
 __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, int64_t j) {
     using V = cplx<T>;
@@ -273,7 +284,7 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
         nrm = v.x * v.x + v.y * v.y;
         // |v|^order: the square root for the magnitude, no power for order 2
         if (s.post_param == 1.0)
-            nrm = sqrt(nrm);
+            nrm = mag_sqrt<T>(nrm);
         else if (s.post_param != 2.0)
             nrm = pow(nrm, (T)(s.post_param * 0.5));
     }
@@ -359,7 +370,7 @@ __device__ __forceinline__ void store_nyquist(const Side& s, int64_t off, cplx<T
     if (s.flags & SF_NORM) {
         r = x.x * x.x + x.y * x.y;
         if (s.post_param == 1.0)
-            r = sqrt(r);
+            r = mag_sqrt<T>(r);
         else if (s.post_param != 2.0)
             r = pow(r, (T)(s.post_param * 0.5));
     }
@@ -506,18 +517,23 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
         const int st = (int)s.ax_stride;
         if (f & SF_RPAIR) {
             // the pair vector load needs the line's address aligned to the pair type
-            const bool vec = st == 1 && (reinterpret_cast<uintptr_t>(lp) % sizeof(V)) == 0;
+            if (!la.ok) {
 #pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const int a = pos(i);
-                V x = cmk<V>(T(0), T(0));
-                if (la.ok) x = vec ? reinterpret_cast<const V*>(lp)[a] : cmk<V>(lp[2 * a * st], lp[(2 * a + 1) * st]);
-                if (wt) {
-                    const V w = __ldg(reinterpret_cast<const V*>(wt) + a);
-                    x.x *= w.x;
-                    x.y *= w.y;
+                for (int i = 0; i < N; ++i) v[i] = cmk<V>(T(0), T(0));
+            } else if (st == 1 && (reinterpret_cast<uintptr_t>(lp) % sizeof(V)) == 0) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) v[i] = reinterpret_cast<const V*>(lp)[pos(i)];
+            } else {
+#pragma unroll
+                for (int i = 0; i < N; ++i) v[i] = cmk<V>(lp[2 * pos(i) * st], lp[(2 * pos(i) + 1) * st]);
+            }
+            if (wt) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) {
+                    const V w = __ldg(reinterpret_cast<const V*>(wt) + pos(i));
+                    v[i].x *= w.x;
+                    v[i].y *= w.y;
                 }
-                v[i] = x;
             }
         } else {
 #pragma unroll
@@ -617,7 +633,7 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
                 if (norm) {
                     r = v[i].x * v[i].x + v[i].y * v[i].y;
                     if (order == T(1))
-                        r = sqrt(r);
+                        r = mag_sqrt<T>(r);
                     else if (order != T(2))
                         r = pow(r, order * T(0.5));
                 }
@@ -831,15 +847,26 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassPara
 }
 
 // Fused Bluestein bodies with 16 elements a thread would take 160-180 registers;
-// k_line_2 holds them to 128 so that two 256-thread CTAs share an SM.  Other bodies
-// keep the register count ptxas picks by itself (any minimum-blocks bound, 1
-// included, lets it spend registers up to the bound).
+// k_line_2 holds them to 128 so that two 256-thread CTAs share an SM.  The float32
+// real-spectrum variants (3, 4, 5) of 256 to 1024 points run four CTAs an SM
+// (k_line_4, 64 registers, a few spilled): the frame-major spectrogram pass went
+// from 59 to 41 us with the paired loads split and the approximate square root.
+// Other bodies keep the register count ptxas picks by itself (any minimum-blocks
+// bound, 1 included, lets it spend registers up to the bound).
 template <typename T, int L, int MODE, int VAR> struct LineMinBlocks {
-    static constexpr int V = (VAR == 1 && Radix<T, L>::RT == 16 && L >= 512 && LineCfg<T, L, MODE>::NT <= 256) ? 2 : 1;
+    static constexpr int V = (VAR == 1 && Radix<T, L>::RT == 16 && L >= 512 && LineCfg<T, L, MODE>::NT <= 256) ? 2
+                             : ((VAR == 3 || VAR == 4 || VAR == 5) && sizeof(T) == 4 && L >= 256 && L <= 1024) ? 4
+                                                                                                                : 1;
 };
 
 template <typename T, int L, int MODE, int VAR>
 __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT, 2) k_line_2(const PassParams p) {
+    extern __shared__ __align__(16) unsigned char rk_smem[];
+    line_body<T, L, MODE, VAR>(p, blockIdx.x, rk_smem, threadIdx.x);
+}
+
+template <typename T, int L, int MODE, int VAR>
+__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT, 4) k_line_4(const PassParams p) {
     extern __shared__ __align__(16) unsigned char rk_smem[];
     line_body<T, L, MODE, VAR>(p, blockIdx.x, rk_smem, threadIdx.x);
 }

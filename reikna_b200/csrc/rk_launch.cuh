@@ -14,6 +14,8 @@ template <typename T, int L, int MODE, int VAR> struct LineLauncher {
     static constexpr auto kernel() {
         if constexpr (LineMinBlocks<T, L, MODE, VAR>::V == 2)
             return &k_line_2<T, L, MODE, VAR>;
+        else if constexpr (LineMinBlocks<T, L, MODE, VAR>::V == 4)
+            return &k_line_4<T, L, MODE, VAR>;
         else
             return &k_line<T, L, MODE, VAR>;
     }
