@@ -29,10 +29,8 @@ struct TmaInfo {
     int nl;
     size_t smem;
 };
-// persistent TMA-fed line pass of length L, mode and variant (0 plain, 3 / 4 the real
-// spectrum step after / before the FFT)
-bool tma_info(int dbl, int L, int mode, int var, TmaInfo* out);
-bool tma_info_real(int dbl, int L, int mode, int var, TmaInfo* out);
+// persistent TMA-fed plain line pass of length L and mode
+bool tma_info(int dbl, int L, int mode, TmaInfo* out);
 bool encode_lane_map(void* base, int dbl, int64_t I, int64_t L, int64_t O, int64_t sj, int64_t so, int nl, int rows,
                      TensorMapBytes* out);
 

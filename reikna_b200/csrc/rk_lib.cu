@@ -702,16 +702,9 @@ static void setup_tma(PassRec& r, int dbl, int nsm) {
     const Side& ld = p.ld;
     const Side& st = p.st;
     const int esz = dbl ? 16 : 8;
-    // sides: the lean block paths; the antiperiodic forward transform's load table
-    // (variant 3) and inverse transform's store table (variant 4) are applied by the
-    // TMA kernel and store_block; the inverse real step reads whole rows of L bins
-    const bool ld_ok = (ld.flags & SF_FAST) ||
-                       (r.var == 3 && (ld.flags & SF_FAST2) && !(ld.flags & ~(SF_FAST2 | SF_TAB | SF_SCALE)) &&
-                        ld.cA == 0 && ld.jB == 1 && ld.ax_len == r.L && ld.ax_bound == r.L);
-    const bool st_ok = (st.flags & SF_FAST) || (r.var == 4 && (st.flags & SF_FAST2));
-    if (!ld_ok || !st_ok || ld.ax_shift != 0 || p.C != 1 || (r.var == 4 && p.rnyq)) return;
+    if (!(ld.flags & SF_FAST) || !(st.flags & SF_FAST) || ld.ax_shift != 0 || p.C != 1) return;
     TmaInfo ti;
-    if (!tma_info(dbl, r.L, r.mode, r.var, &ti)) return;
+    if (!tma_info(dbl, r.L, r.mode, &ti)) return;
     const int64_t L = r.L, NL = ti.nl;
     for (int i = 0; i < ld.nd_o; ++i)
         if (ld.o_shift[i] != 0 || ld.o_bound[i] != ld.o_shape[i]) return;
@@ -1214,7 +1207,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             }
             r.nblocks = (pp.nlines + li.nl - 1) / li.nl;
             r.li = li;
-            if (!(desc->flags & RK_FLAG_NO_TMA) && (ps.var == 0 || ps.var == 3 || ps.var == 4)) setup_tma(r, dbl, nsm);
+            if (!(desc->flags & RK_FLAG_NO_TMA) && ps.var == 0) setup_tma(r, dbl, nsm);
             if ((desc->flags & RK_FLAG_SPLIT_TC) && tc_eligible(r)) {
                 r.use_tc = true;
                 r.use_tma = false;

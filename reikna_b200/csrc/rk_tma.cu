@@ -21,11 +21,9 @@
 namespace rk {
 
 #define RK_TI(TY, LL, MODE) \
-    if (L == LL && mode == MODE) { *out = TmaLauncher<TY, LL, MODE, 0>::info(); return true; }
+    if (L == LL && mode == MODE) { *out = TmaLauncher<TY, LL, MODE>::info(); return true; }
 
-bool tma_info(int dbl, int L, int mode, int var, TmaInfo* out) {
-    if (var == 3 || var == 4) return tma_info_real(dbl, L, mode, var, out);
-    if (var != 0) return false;
+bool tma_info(int dbl, int L, int mode, TmaInfo* out) {
     if (!dbl) {
         RK_TI(float, 64, MODE_POS)
         RK_TI(float, 128, MODE_POS)

@@ -1,5 +1,4 @@
-// Persistent TMA-fed line pass (the kernel template; instantiated by rk_tma.cu for
-// plain passes and by rk_tma_real.cu for the one-pass real transforms).
+// Persistent TMA-fed line pass (the kernel template; instantiated by rk_tma.cu).
 #pragma once
 #include "rk_async.cuh"
 #include "rk_internal.h"
@@ -15,7 +14,7 @@ template <typename T, int L, int MODE> struct TmaCfg {
     static constexpr size_t SMEM = 2 * (size_t)BUF * ESZ + 64;                     // + 2 mbarriers
 };
 
-template <typename T, int L, int MODE, int VAR>
+template <typename T, int L, int MODE>
 __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line_tma(const __grid_constant__ PassParams p) {
     using V = cplx<T>;
     using E = Engine<T, L, MODE>;
@@ -76,103 +75,49 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line_tma(const __gr
             break;
         }
         V v[RT];
-        if constexpr (VAR == 4) {
-            // inverse real transforms (rows of L bins, no Nyquist bin on this path): the
-            // half-length spectrum from the tile pair by pair, reordered through the
-            // buffer into the FFT's input order
-            static_assert(MODE == MODE_POS, "the real-signal step needs whole lines");
 #pragma unroll
-            for (int i = 0; i < RT; ++i) v[i] = edge_value<T>(p.ld, buf[ln * L + pair_pos<L, RT, TPL>(tb, i, p.rodd)]);
-            real_pairs_in<T, L, RT, TPL>(p, tb, cmk<V>(T(0), T(0)), v);
-            __syncthreads();
+        for (int z = 0; z < RT / R0; ++z)
 #pragma unroll
-            for (int i = 0; i < RT; ++i) buf[E::sidx(ln, pair_pos<L, RT, TPL>(tb, i, p.rodd))] = v[i];
-            __syncthreads();
-#pragma unroll
-            for (int z = 0; z < RT / R0; ++z)
-#pragma unroll
-                for (int m = 0; m < R0; ++m) v[z * R0 + m] = buf[E::sidx(ln, E::in_pos(tb, z, m))];
-        } else {
-#pragma unroll
-            for (int z = 0; z < RT / R0; ++z)
-#pragma unroll
-                for (int m = 0; m < R0; ++m) {
-                    const int pos = E::in_pos(tb, z, m);
-                    v[z * R0 + m] = MODE == MODE_POS ? buf[ln * L + pos] : buf[pos * NL + ln];
-                }
-            const int32_t f = p.ld.flags;
-            if (f & SF_SCALE) scale_block<T, RT>(p.ld, v);
-            if (f & SF_TAB) {
-                // a per-position table (the antiperiodic forward transform's W_2L^m),
-                // between the two conjugations as in the element path
-                if (f & SF_PRE_CONJ) {
-#pragma unroll
-                    for (int i = 0; i < RT; ++i) v[i].y = -v[i].y;
-                }
-                const V* tab = reinterpret_cast<const V*>(p.ld.tab);
-#pragma unroll
-                for (int z = 0; z < RT / R0; ++z)
-#pragma unroll
-                    for (int m = 0; m < R0; ++m) v[z * R0 + m] = cmul(v[z * R0 + m], __ldg(tab + E::in_pos(tb, z, m)));
-                if (f & SF_POST_CONJ) {
-#pragma unroll
-                    for (int i = 0; i < RT; ++i) v[i].y = -v[i].y;
-                }
-            } else if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
-#pragma unroll
-                for (int i = 0; i < RT; ++i) v[i].y = -v[i].y;
+            for (int m = 0; m < R0; ++m) {
+                const int pos = E::in_pos(tb, z, m);
+                v[z * R0 + m] = MODE == MODE_POS ? buf[ln * L + pos] : buf[pos * NL + ln];
             }
+        if (p.ld.flags & SF_SCALE) scale_block<T, RT>(p.ld, v);
+        if (((p.ld.flags & SF_PRE_CONJ) != 0) != ((p.ld.flags & SF_POST_CONJ) != 0)) {
+#pragma unroll
+            for (int i = 0; i < RT; ++i) v[i].y = -v[i].y;
         }
         __syncthreads();  // the tile is in registers: the buffer becomes the exchange area
         E::run(v, buf, ln, tb, tw);
         if constexpr (E::NS == 1) __syncthreads();
-        V nyq = cmk<V>(T(0), T(0));
-        if constexpr (VAR == 3) {
-            // real-signal spectrum X[k] = Z[k] A_k + conj(Z[mirror k]) B_k through the
-            // exchange buffer, before the next copy lands in it
-            static_assert(MODE == MODE_POS, "the real-spectrum step needs whole lines");
-#pragma unroll
-            for (int z = 0; z < RT / RL; ++z)
-#pragma unroll
-                for (int m = 0; m < RL; ++m) buf[E::sidx(ln, E::out_pos(tb, z, m))] = v[z * RL + m];
-            __syncthreads();
-            nyq = real_pairs_out<T, L, RT, TPL>(p, tb, [&](int k) { return buf[E::sidx(ln, k)]; }, v);
-            __syncthreads();
-        }
         if (tid == 0 && t + 2 * stride < p.ntiles) {
             fence_proxy_async_smem();
             issue(t + 2 * stride, b);
         }
         const int64_t line = t * NL + ln;
         const LineAddr la = line_addr(p.st, line, p.C, p.I, line < p.nlines);
-        if constexpr (VAR == 3) {
-            if (p.rnyq && tb == 0 && la.ok) store_nyquist<T>(p.st, la.base + (int64_t)L * p.st.ax_stride, nyq);
-        }
-        if constexpr (VAR == 3)
-            store_block<T, RT>(p.st, p, la, [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
-        else
-            store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
+        store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
     }
 }
 
-template <typename T, int L, int MODE, int VAR> struct TmaLauncher {
+template <typename T, int L, int MODE> struct TmaLauncher {
     using C = TmaCfg<T, L, MODE>;
     static cudaError_t launch(const PassParams& p, int64_t nblocks, cudaStream_t st) {
         static bool attr_done = false;
         if (!attr_done) {
             cudaError_t e =
-                cudaFuncSetAttribute(k_line_tma<T, L, MODE, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+                cudaFuncSetAttribute(k_line_tma<T, L, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
             if (e != cudaSuccess) return e;
             attr_done = true;
         }
         if (nblocks <= 0) return cudaSuccess;
-        k_line_tma<T, L, MODE, VAR><<<(unsigned)nblocks, C::NT, C::SMEM, st>>>(p);
+        k_line_tma<T, L, MODE><<<(unsigned)nblocks, C::NT, C::SMEM, st>>>(p);
         return cudaGetLastError();
     }
     static int per_sm() {
         int n = 0;
-        cudaFuncSetAttribute(k_line_tma<T, L, MODE, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_line_tma<T, L, MODE, VAR>, C::NT, C::SMEM);
+        cudaFuncSetAttribute(k_line_tma<T, L, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_line_tma<T, L, MODE>, C::NT, C::SMEM);
         return n;
     }
     static TmaInfo info() { return TmaInfo{&launch, &per_sm, C::NT, C::NL, C::SMEM}; }
