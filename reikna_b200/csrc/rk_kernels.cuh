@@ -272,7 +272,6 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
     if (f & SF_PRE_CONJ) v = cconj(v);
     if (!(la.ok && a < s.ax_len)) return;
     if (f & SF_CHIRP) v = cmul(v, reinterpret_cast<const V*>(s.chirp)[a]);
-    if (f & SF_TAB) v = cmul(v, reinterpret_cast<const V*>(s.tab)[a]);
     if (f & SF_POST_CONJ) v = cconj(v);
     if (f & SF_SCALE) v = cmul(v, cmk<V>((T)s.scale_re, (T)s.scale_im));
     int64_t u = a + s.ax_shift;
@@ -591,14 +590,6 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
                 if (a < alen) v[i] = cmul(v[i], __ldg(ch + a));
             }
         }
-        if (f & SF_TAB) {
-            const V* tb = reinterpret_cast<const V*>(s.tab);
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const int a = a0 + pos(i) * jB;
-                if (a < alen) v[i] = cmul(v[i], __ldg(tb + a));
-            }
-        }
         if (f & SF_POST_CONJ) {
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
@@ -770,6 +761,17 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
         }
     }
     E::run(v, sm, ln, tb, tw);
+    if constexpr (VAR == 4) {
+        // antiperiodic inverse: W_2L^m on the FFT's output, which the store then
+        // conjugates (the inverse's last conjugation) into W_2L^-m on the result
+        if (p.rtwid) {
+            const V* tt = reinterpret_cast<const V*>(p.rtwid);
+#pragma unroll
+            for (int z = 0; z < RT / RL; ++z)
+#pragma unroll
+                for (int m = 0; m < RL; ++m) v[z * RL + m] = cmul(v[z * RL + m], __ldg(tt + E::out_pos(tb, z, m)));
+        }
+    }
     if constexpr (VAR == 1) {
         // multiply by the kernel spectrum (1/M folded in) and conjugate, so that a
         // second forward FFT followed by a conjugation yields the inverse FFT

@@ -1084,10 +1084,11 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         pp.nlines = ps.O * ps.C * ps.I;
         build_side(*desc, ps.ld, ps.axis, dbl, true, pp.ld);
         build_side(*desc, ps.st, ps.kind == PK_PLANE ? ps.axis2 : ps.axis, dbl, false, pp.st);
-        // antiperiodic transforms: W_2L^m on the first load (forward) or, conjugated
-        // by the inverse's last conjugation, on the last store
+        // antiperiodic transforms: W_2L^m on the first load (forward, a load-side
+        // table) or after the FFT of the inverse (variant 4's rtwid), which the last
+        // store's conjugation turns into W_2L^-m
         const bool ap_tab = (ps.var == 3 || ps.var == 4) && (desc->flags & RK_FLAG_ANTIPERIODIC);
-        if (ap_tab) (ps.var == 3 ? pp.ld : pp.st).flags |= SF_TAB;
+        if (ap_tab && ps.var == 3) pp.ld.flags |= SF_TAB;
         mark_fast(pp.ld, dbl, ps.kind == PK_PLANE ? ps.L2 : ps.L);
         mark_fast(pp.st, dbl, ps.kind == PK_PLANE ? ps.L1 : ps.L);
         mark_fast2(pp.ld, dbl, ps.kind == PK_PLANE ? ps.L2 : ps.L, ps.C);
@@ -1146,7 +1147,10 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
                 k_gen_rpost<<<(unsigned)((L + 256) / 256), 256>>>(L, dbl ? nullptr : (float2*)tt,
                                                                   dbl ? (double2*)tt : nullptr);
                 CK(cudaGetLastError());
-                (ps.var == 3 ? pp.ld : pp.st).tab = tt;
+                if (ps.var == 3)
+                    pp.ld.tab = tt;
+                else
+                    pp.rtwid = tt;
             }
         }
         if (ps.ld.chirp_axis >= 0) {

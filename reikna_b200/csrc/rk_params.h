@@ -83,6 +83,7 @@ struct PassParams {
     // mirror k = (L - k - rodd) mod L; rnyq: the bin L is also stored (var 3) or
     // read as the mirror of bin 0 (var 4)
     const void* rmix;
+    const void* rtwid;  // antiperiodic inverse (variant 4): W_2L^m applied after the FFT
     double rh;
     int32_t rodd, rnyq;
 };

@@ -82,7 +82,11 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line_tma(const __gr
                 const int pos = E::in_pos(tb, z, m);
                 v[z * R0 + m] = MODE == MODE_POS ? buf[ln * L + pos] : buf[pos * NL + ln];
             }
-        if (p.ld.flags & SF_SCALE) scale_block<T, RT>(p.ld, v);
+        if (p.ld.flags & SF_SCALE) {
+            const V c = cmk<V>((T)p.ld.scale_re, (T)p.ld.scale_im);
+#pragma unroll
+            for (int i = 0; i < RT; ++i) v[i] = cmul(v[i], c);
+        }
         if (((p.ld.flags & SF_PRE_CONJ) != 0) != ((p.ld.flags & SF_POST_CONJ) != 0)) {
 #pragma unroll
             for (int i = 0; i < RT; ++i) v[i].y = -v[i].y;
