@@ -175,7 +175,9 @@ template <> __device__ __forceinline__ float mag_sqrt<float>(float x) {
     return r;
 }
 
-template <typename T>
+// RP: compile the pair-read branch in (only the half-length route's passes set
+// SF_RPAIR; other kernels leave it out to keep their registers)
+template <typename T, bool RP = true>
 __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, int64_t j) {
     using V = cplx<T>;
     V v = cmk<V>(T(0), T(0));
@@ -183,7 +185,7 @@ __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, 
     if (la.ok && a < s.ax_len) {
         int64_t u = a + s.ax_shift;
         if (u >= s.ax_len) u -= s.ax_len;
-        if ((s.flags & SF_RPAIR) && u < s.ax_bound) {
+        if (RP && (s.flags & SF_RPAIR) && u < s.ax_bound) {
             // a real signal read as sample pairs (x[2u], x[2u+1]); a window covers the
             // sample index 2u / 2u + 1
             const int64_t off = la.base + 2 * u * s.ax_stride;
@@ -324,18 +326,9 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
 // two multiplications an element instead of a complex product (same results)
 template <typename T, int N>
 __device__ __forceinline__ void scale_block(const Side& s, cplx<T>* v) {
-    if (s.scale_im == 0.0) {
-        const T r = (T)s.scale_re;
+    const cplx<T> c = cmk<cplx<T>>((T)s.scale_re, (T)s.scale_im);
 #pragma unroll
-        for (int i = 0; i < N; ++i) {
-            v[i].x *= r;
-            v[i].y *= r;
-        }
-    } else {
-        const cplx<T> c = cmk<cplx<T>>((T)s.scale_re, (T)s.scale_im);
-#pragma unroll
-        for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
-    }
+    for (int i = 0; i < N; ++i) v[i] = cmul(v[i], c);
 }
 
 // The value ops of a pass-dtype side without tables, for an element read outside the
@@ -450,7 +443,7 @@ __device__ __forceinline__ void real_pairs_in(const PassParams& p, int tb, cplx<
     }
 }
 
-template <typename T, int N, class PosF>
+template <typename T, int N, bool RP = true, class PosF>
 __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, PosF pos, cplx<T>* v) {
     using V = cplx<T>;
     const int32_t f = s.flags;
@@ -514,7 +507,7 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
         const T* lp = reinterpret_cast<const T*>(s.ptr) + la.base;
         const T* wt = (f & SF_WINDOW) ? reinterpret_cast<const T*>(s.win) : nullptr;
         const int st = (int)s.ax_stride;
-        if (f & SF_RPAIR) {
+        if (RP && (f & SF_RPAIR)) {
             // the pair vector load needs the line's address aligned to the pair type
             if (!la.ok) {
 #pragma unroll
@@ -550,16 +543,21 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
         }
     } else {
 #pragma unroll
-        for (int i = 0; i < N; ++i) v[i] = side_load<T>(s, la, pos(i));
+        for (int i = 0; i < N; ++i) v[i] = side_load<T, RP>(s, la, pos(i));
     }
 }
 
-template <typename T, int N, class PosF>
+// PATHS: the lean paths compiled in (STORE_FAST | STORE_FAST2 | STORE_FASTR); a side
+// marked for a path left out takes the general element path.  Kernels whose store
+// sides only ever take SF_FAST compile the others out to keep their registers.
+enum : int { STORE_FAST = 1, STORE_FAST2 = 2, STORE_FASTR = 4, STORE_ALL = 7 };
+
+template <typename T, int N, int PATHS = STORE_ALL, class PosF>
 __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, const LineAddr& la, PosF pos,
                                             cplx<T>* v) {
     using V = cplx<T>;
     const int32_t f = s.flags;
-    if (f & SF_FAST) {
+    if ((PATHS & STORE_FAST) && (f & SF_FAST)) {
         if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
@@ -571,7 +569,7 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
 #pragma unroll
             for (int i = 0; i < N; ++i) lp[((pos(i) + sh) & mask) * st] = v[i];
         }
-    } else if (f & SF_FAST2) {
+    } else if ((PATHS & STORE_FAST2) && (f & SF_FAST2)) {
         const int a0 = (int)(la.c * s.cA), jB = (int)s.jB, st = (int)s.ax_stride;
         const int bound = (int)s.ax_bound, alen = (int)s.ax_len;
         if (f & SF_TW4) {
@@ -603,7 +601,7 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
                 if (a < bound) lp[a * st] = v[i];
             }
         }
-    } else if (f & SF_FASTR) {
+    } else if ((PATHS & STORE_FASTR) && (f & SF_FASTR)) {
         // real output of the pass precision (real part or |v|^order, e.g. magnitudes),
         // positions at or beyond the axis bound are cropped
         if (((f & SF_PRE_CONJ) != 0) != ((f & SF_POST_CONJ) != 0)) {
@@ -744,7 +742,7 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
             // by pair; with rnyq the mirror of bin 0 is bin L of the input row, and
             // bins 0 and L lose their imaginary parts
             static_assert(MODE == MODE_POS, "the real-signal step needs whole lines");
-            load_block<T, RT>(p.ld, la, [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
+            load_block<T, RT, false>(p.ld, la, [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
             V yl = cmk<V>(T(0), T(0));
             if (p.rnyq && la.ok) yl = edge_value<T>(p.ld, reinterpret_cast<const V*>(p.ld.ptr)[la.base + (int64_t)L * p.ld.ax_stride]);
             real_pairs_in<T, L, RT, TPL>(p, tb, yl, v);
@@ -757,7 +755,8 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
                 for (int m = 0; m < R0; ++m) v[z * R0 + m] = sm[E::sidx(ln, E::in_pos(tb, z, m))];
             __syncthreads();
         } else {
-            load_block<T, RT>(p.ld, la, [&](int i) { return E::in_pos(tb, i / R0, i % R0); }, v);
+            // sample-pair reads (SF_RPAIR) only occur on the half-length route's passes
+            load_block<T, RT, VAR == 3 || VAR == 5>(p.ld, la, [&](int i) { return E::in_pos(tb, i / R0, i % R0); }, v);
         }
     }
     E::run(v, sm, ln, tb, tw);

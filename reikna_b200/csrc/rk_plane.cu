@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, PlaneCfg<T, L1, L2
     {
         const int64_t line = plane * L1 + (int64_t)q * C::NLR + ln;
         const LineAddr la = line_addr(p.ld, line, 1, 1, pok);
-        load_block<T, RT>(p.ld, la, [&](int i) { return ER::in_pos(tb, i / ER::R0, i % ER::R0); }, v);
+        load_block<T, RT, false>(p.ld, la, [&](int i) { return ER::in_pos(tb, i / ER::R0, i % ER::R0); }, v);
         ER::run(v, sm, ln, tb, tw);
     }
     if constexpr (Q > 1)
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, PlaneCfg<T, L1, L2
     {
         const int64_t line = plane * L2 + col;
         const LineAddr la = line_addr(p.st, line, 1, L2, pok);
-        store_block<T, RT>(p.st, p, la, [&](int i) { return EC::out_pos(tc, i / EC::RL, i % EC::RL); }, v);
+        store_block<T, RT, STORE_FAST>(p.st, p, la, [&](int i) { return EC::out_pos(tc, i / EC::RL, i % EC::RL); }, v);
     }
 }
 
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, (PlaneTmaCfg<T, L1
             if (!last && tid < Q) mbar_arrive_remote(mapa(empty_s, (uint32_t)tid));
         const int64_t line = plane * L2 + q * C::NLC + lc;
         const LineAddr la = line_addr(p.st, line, 1, L2, true);
-        store_block<T, RT>(p.st, p, la, [&](int i) { return EC::out_pos(tc, i / EC::RL, i % EC::RL); }, v);
+        store_block<T, RT, STORE_FAST>(p.st, p, la, [&](int i) { return EC::out_pos(tc, i / EC::RL, i % EC::RL); }, v);
     }
     if (!healthy) mbar_wait(&bars[0], pa, nullptr);
     // no CTA leaves while another could still address its shared memory

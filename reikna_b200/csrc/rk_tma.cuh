@@ -100,7 +100,8 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line_tma(const __gr
         }
         const int64_t line = t * NL + ln;
         const LineAddr la = line_addr(p.st, line, p.C, p.I, line < p.nlines);
-        store_block<T, RT>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
+        // the planner takes this kernel only for SF_FAST store sides
+        store_block<T, RT, STORE_FAST>(p.st, p, la, [&](int i) { return E::out_pos(tb, i / RL, i % RL); }, v);
     }
 }
 
