@@ -443,11 +443,15 @@ __device__ __forceinline__ void real_pairs_in(const PassParams& p, int tb, cplx<
     }
 }
 
-template <typename T, int N, bool RP = true, class PosF>
+// LPATHS: the lean load paths compiled in (LOAD_FAST | LOAD_FAST2 | LOAD_FASTR); RP:
+// the sample-pair reads.  A side marked for a path left out takes the general path.
+enum : int { LOAD_FAST = 1, LOAD_FAST2 = 2, LOAD_FASTR = 4, LOAD_ALL = 7 };
+
+template <typename T, int N, bool RP = true, int LPATHS = LOAD_ALL, class PosF>
 __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, PosF pos, cplx<T>* v) {
     using V = cplx<T>;
     const int32_t f = s.flags;
-    if (f & SF_FAST) {
+    if ((LPATHS & LOAD_FAST) && (f & SF_FAST)) {
         const V* lp = reinterpret_cast<const V*>(s.ptr) + la.base;
         const int st = (int)s.ax_stride, sh = s.ax_shift, mask = (int)s.ax_len - 1;
         if (la.ok) {
@@ -462,7 +466,7 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
         }
-    } else if (f & SF_FAST2) {
+    } else if ((LPATHS & LOAD_FAST2) && (f & SF_FAST2)) {
         // pass-dtype side with an index map a = c cA + j jB (four-step, Bluestein
         // padding): one line pointer, 32-bit offsets, a bounds predicate, and the
         // chirp / table ops in side_load's order
@@ -499,7 +503,7 @@ __device__ __forceinline__ void load_block(const Side& s, const LineAddr& la, Po
 #pragma unroll
             for (int i = 0; i < N; ++i) v[i].y = -v[i].y;
         }
-    } else if (f & SF_FASTR) {
+    } else if ((LPATHS & LOAD_FASTR) && (f & SF_FASTR)) {
         // real input of the pass precision (e.g. windowed signal frames): one line
         // pointer, 32-bit offsets, the window from the plan's table; SF_RPAIR reads the
         // samples 2a and 2a + 1 as one element (one vector load on a contiguous,
@@ -756,7 +760,11 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
             __syncthreads();
         } else {
             // sample-pair reads (SF_RPAIR) only occur on the half-length route's passes
-            load_block<T, RT, VAR == 3 || VAR == 5>(p.ld, la, [&](int i) { return E::in_pos(tb, i / R0, i % R0); }, v);
+            // (variants 5 and 6, whose loads are always real); the complex-input
+            // real-spectrum pass (variant 3) never meets a real side
+            constexpr bool half = VAR == 5 || VAR == 6;
+            constexpr int lp = half ? LOAD_FASTR : (VAR == 3 ? (LOAD_FAST | LOAD_FAST2) : LOAD_ALL);
+            load_block<T, RT, half, lp>(p.ld, la, [&](int i) { return E::in_pos(tb, i / R0, i % R0); }, v);
         }
     }
     E::run(v, sm, ln, tb, tw);
@@ -790,7 +798,7 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
         __syncthreads();
         E::run(v, sm, ln, tb, tw);
     }
-    if constexpr (VAR == 3 || VAR == 5) {
+    if constexpr (VAR == 3 || VAR == 5 || VAR == 6) {
         // real-signal spectrum from the half-length spectrum Z of this line (the line
         // holds x[2n] + i x[2n+1]): X[k] = Z[k] A_k + conj(Z[mirror k]) B_k with the
         // plan's FP64-generated w_k in rmix; with rnyq the Nyquist bin
@@ -805,7 +813,7 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
         const V nyq = real_pairs_out<T, L, RT, TPL>(p, tb, [&](int k) { return sm[E::sidx(ln, k)]; }, v);
         const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
         if (tb == 0 && la.ok && p.rnyq) store_nyquist<T>(p.st, la.base + (int64_t)L * p.st.ax_stride, nyq);
-        if constexpr (VAR == 3) {
+        if constexpr (VAR == 3 || VAR == 6) {
             store_block<T, RT>(p.st, p, la, [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
         } else {
             __syncthreads();
@@ -849,14 +857,14 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassPara
 
 // Fused Bluestein bodies with 16 elements a thread would take 160-180 registers;
 // k_line_2 holds them to 128 so that two 256-thread CTAs share an SM.  The float32
-// real-spectrum variants (3, 4, 5) of 256 to 1024 points run four CTAs an SM
+// real-spectrum variants (3 to 6) of 256 to 1024 points run four CTAs an SM
 // (k_line_4, 64 registers, a few spilled): the frame-major spectrogram pass went
 // from 59 to 41 us with the paired loads split and the approximate square root.
 // Other bodies keep the register count ptxas picks by itself (any minimum-blocks
 // bound, 1 included, lets it spend registers up to the bound).
 template <typename T, int L, int MODE, int VAR> struct LineMinBlocks {
     static constexpr int V = (VAR == 1 && Radix<T, L>::RT == 16 && L >= 512 && LineCfg<T, L, MODE>::NT <= 256) ? 2
-                             : ((VAR == 3 || VAR == 4 || VAR == 5) && sizeof(T) == 4 && L >= 256 && L <= 1024) ? 4
+                             : (VAR >= 3 && sizeof(T) == 4 && L >= 256 && L <= 1024)                          ? 4
                                                                                                                 : 1;
 };
 

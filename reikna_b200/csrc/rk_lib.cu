@@ -281,7 +281,7 @@ static int64_t prod_range(const int64_t* s, int a, int b) {
 // real_to_complex + crop_frequencies), N/2 a power of two one pass covers: the
 // half-length route applies.  Any conjugation or scale of the input is folded into
 // the output per call (the input is real, the transform linear).
-// Returns the line-pass variant: 3 (bins stored along the line), 5 (a transposed
+// Returns the line-pass variant: 6 (bins stored along the line), 5 (a transposed
 // output whose lines are adjacent in memory: bins stored lane-fastest), 0 = no.
 static int half_eligible(const rk_fft_desc& d, int dbl) {
     if (d.flags & (RK_FLAG_NO_HALF | RK_FLAG_REAL_POST | RK_FLAG_REAL_PRE)) return 0;
@@ -298,7 +298,7 @@ static int half_eligible(const rk_fft_desc& d, int dbl) {
     if (in.window != RK_WIN_NONE && in.window_axis != ax) return 0;
     if (out.shift[ax] != 0 || out.shape[ax] > L + 1) return 0;
     if (!(out.format == cfmt || (out.format == rfmt && out.post == RK_POST_NORM))) return 0;
-    if (out.strides[ax] == 1) return 3;
+    if (out.strides[ax] == 1) return 6;
     if (ax > 0 && out.strides[ax - 1] == 1 && d.shape[ax - 1] > 1 && L <= lane_max(dbl)) return 5;
     return 0;
 }
@@ -1111,7 +1111,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             mark_fastr(pp.ld, dbl, ps.L, true);
             mark_fastr(pp.st, dbl, ps.L, false);
         }
-        if (ps.var == 3 || ps.var == 4 || ps.var == 5) {
+        if (ps.var >= 3 && ps.var <= 6) {
             const int cfmt = dbl ? RK_FMT_C128 : RK_FMT_C64, rfmt = dbl ? RK_FMT_F64 : RK_FMT_F32;
             const bool edges_ok = (pp.ld.flags & SF_RPAIR)
                                       ? (pp.ld.fmt == rfmt &&

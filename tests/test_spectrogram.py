@@ -25,7 +25,7 @@ def test_transposed_spectrogram_plans_a_lane_fastest_store():
     # real-spectrum step and the magnitude in its store
     d = spectrogram(2**14, 256, 64).describe()
     p = d["passes"]
-    assert len(p) == 1 and p[0]["note"] == "half" and p[0]["var"] == 3 and p[0]["L"] == 128
+    assert len(p) == 1 and p[0]["note"] == "half" and p[0]["var"] == 6 and p[0]["L"] == 128
 
 
 def test_transpose_2d_shape_and_errors():
