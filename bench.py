@@ -664,7 +664,7 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> int:
             cc(None, o, i)
 
     res = {"plain_per_call": {"us": timed(plain, reps) * 1e3}}
-    for mode in ("calls", "graph", "persistent", "auto"):
+    for mode in ("calls", "graph", "graph_par", "persistent", "auto"):
         bat = BatchedFFT(comps, device=dev, mode=mode)
         ms = timed(lambda: bat(None, args_list), reps)
         errs = [float(numpy.linalg.norm((o.cpu().numpy() - r).ravel()) / numpy.linalg.norm(r.ravel())) for o, r in zip(outs, refs)]

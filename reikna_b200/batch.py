@@ -10,6 +10,11 @@ connected transformations) as one unit, in one of three modes:
 ``"graph"``
     the same launches captured once into a CUDA graph and replayed (one graph launch
     per call; recaptured when the argument pointers change);
+``"graph_par"``
+    as ``"graph"``, with every member on its own branch of the graph (forked from
+    and joined back to the calling stream), so the kernels of independent members
+    run concurrently and a member that leaves SMs idle (a one-CTA-an-SM Bluestein
+    pass, a short final wave) shares them with the others;
 ``"persistent"``
     ``rk_batch_execute``: one persistent kernel whose CTAs pull the tiles of every
     member's passes from a dependency-ordered task list, so small members fill the
@@ -30,7 +35,10 @@ from pathlib import Path
 
 from . import _native as N
 
-MODES = ("calls", "graph", "persistent")
+MODES = ("calls", "graph", "graph_par", "persistent")
+
+# bumped when the candidate set changes, so that older cached choices are re-tuned
+_TUNE_VERSION = b"2"
 
 
 def _cache_path() -> Path:
@@ -39,7 +47,7 @@ def _cache_path() -> Path:
 
 
 def _desc_key(descs) -> str:
-    h = hashlib.sha256()
+    h = hashlib.sha256(_TUNE_VERSION)
     for d in descs:
         h.update(bytes(d))
     return h.hexdigest()[:32]
@@ -71,10 +79,12 @@ class _Variant:
     def __init__(self, comps, device, mode: str, flags: int):
         self.mode = mode
         self.flags = flags
+        self.device = device
         self.callables = [c.compile(device, flags=flags) for c in comps]
         self.plans = [c._runner.plan for c in self.callables]
         self.batch = N.Batch(self.plans) if mode == "persistent" else None
         self._graphs = {}
+        self._branches = None
 
     def bind(self, args_list):
         calls = []
@@ -87,8 +97,26 @@ class _Variant:
         return calls
 
     def _launch_calls(self, calls, stream: int) -> None:
+        if self.mode == "graph_par":
+            self._launch_branches(calls)
+            return
         for plan, (outs, ins, inverse, scalars) in zip(self.plans, calls):
             plan.execute(outs, ins, inverse=inverse, scalars=scalars, stream=stream)
+
+    def _launch_branches(self, calls) -> None:
+        """Each member on its own stream, forked from and joined back to the current
+        torch stream (the capture stream while a graph is captured).  Members are
+        distinct plans with their own temporaries, so they may run at once."""
+        import torch
+
+        if self._branches is None:
+            self._branches = [torch.cuda.Stream(device=self.device) for _ in self.plans]
+        main = torch.cuda.current_stream(self.device)
+        for s, plan, (outs, ins, inverse, scalars) in zip(self._branches, self.plans, calls):
+            s.wait_stream(main)
+            plan.execute(outs, ins, inverse=inverse, scalars=scalars, stream=s.cuda_stream)
+        for s in self._branches:
+            main.wait_stream(s)
 
     def run(self, calls, stream: int) -> None:
         if self.mode == "persistent":
@@ -134,7 +162,7 @@ class BatchedFFT:
     :param computations: ``reikna_b200`` computations (e.g. ``FFT`` objects with
         transformations connected), not yet compiled.
     :param device: torch device (default: the current CUDA device).
-    :param mode: ``"calls"``, ``"graph"``, ``"persistent"`` or ``"auto"``.
+    :param mode: ``"calls"``, ``"graph"``, ``"graph_par"``, ``"persistent"`` or ``"auto"``.
     :param flags: plan flags for a fixed mode (``"persistent"`` adds
         ``FLAG_NO_PLANE``, since plane passes have no batched variant).
 
@@ -168,6 +196,8 @@ class BatchedFFT:
     def candidates(self):
         """(mode, flags) pairs the autotuner tries."""
         out = [("calls", 0), ("calls", N.FLAG_NO_TMA), ("graph", 0), ("graph", N.FLAG_NO_TMA)]
+        if len(self.computations) > 1:
+            out += [("graph_par", 0), ("graph_par", N.FLAG_NO_TMA)]
         out.append(("persistent", N.FLAG_NO_PLANE))
         return out
 

@@ -79,7 +79,7 @@ def test_batch_key_depends_on_members():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["persistent", "graph", "calls"])
+@pytest.mark.parametrize("mode", ["persistent", "graph", "graph_par", "calls"])
 def test_batch_matches_single_calls(mode):
     import torch
 
