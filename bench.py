@@ -5,7 +5,11 @@ Workload (the configuration the headline metric is quoted on): 3-D C2C FFT over 
 axes of a 256 x 256 x 256 complex64 array with a fused output fftshift and 1/N
 scaling transformation.  One step = one forward transform of one array resident in
 HBM; inputs are 134 MB each (larger than the 126 MB L2) and two input/output sets
-alternate between steps.
+alternate between steps.  Consecutive steps are independent and alternate between two
+streams (one compiled plan each), so a step's first pass overlaps the previous step's
+second pass; ``ms_per_step_one_stream`` reports the same steps run back to back on
+one stream, and the roofline's per-kernel durations come from CUDA events around
+every launch in a separate single-stream loop.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl own|reference]
 
@@ -50,7 +54,7 @@ CONFIG = {
     "axes": [0, 1, 2],
     "transformations": ["fftshift (output)", "mul_const 1/N (output)"],
     "bytes_per_step_algorithmic": B_ALG,
-    "l2": "inputs larger than L2 (134 MB each), two buffer sets alternate",
+    "l2": "inputs larger than L2 (134 MB each), two buffer sets alternate (one per stream)",
 }
 
 
@@ -228,44 +232,77 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
     xs = [torch.complex(torch.randn(SHAPE, device=dev, generator=gen), torch.randn(SHAPE, device=dev, generator=gen)) for _ in range(2)]
     outs = [torch.empty_like(xs[0]) for _ in range(2)]
 
-    fft = FFT(xs[0])
-    sh = tr.fftshift(xs[0])
-    sc = tr.mul_const(xs[0], 1.0 / NTOT)
-    fft.parameter.output.connect(sh, sh.input, shifted=sh.output)
-    fft.parameter.shifted.connect(sc, sc.input, result=sc.output)
-    comp = fft.compile(dev)
+    def build():
+        fft = FFT(xs[0])
+        sh = tr.fftshift(xs[0])
+        sc = tr.mul_const(xs[0], 1.0 / NTOT)
+        fft.parameter.output.connect(sh, sh.input, shifted=sh.output)
+        fft.parameter.shifted.connect(sc, sc.input, result=sc.output)
+        return fft.compile(dev)
+
+    # consecutive steps are independent transforms of alternating buffer sets: step k
+    # runs on stream k % 2 with its own compiled plan (each plan owns the intermediate
+    # between its two passes), so one step's plane pass overlaps the previous step's
+    # lane pass
+    comps = [build(), build()]
+    comp = comps[0]
     plan = comp._runner.plan
     launches = plan.launches
     passes = plan.describe()["passes"]
 
     stream = torch.cuda.current_stream(dev)
+    lanes = [torch.cuda.Stream(dev) for _ in range(2)]
     for k in range(args.warmup):
-        comp(stream, outs[k % 2], xs[k % 2])
+        comps[k % 2](lanes[k % 2], outs[k % 2], xs[k % 2])
     torch.cuda.synchronize(dev)
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    plan.profile(args.steps)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local_rank) as clk:
         barrier()
         torch.cuda.synchronize(dev)
         start.record(stream)
+        for s in lanes:
+            s.wait_stream(stream)
         for k in range(args.steps):
-            comp(stream, outs[k % 2], xs[k % 2])
+            comps[k % 2](lanes[k % 2], outs[k % 2], xs[k % 2])
+        for s in lanes:
+            stream.wait_stream(s)
         end.record(stream)
         torch.cuda.synchronize(dev)
         barrier()
     ms = start.elapsed_time(end)
-    pass_ms, calls = plan.profile_read()
-    plan.profile(0)
     if dist is not None:
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * B_ALG * args.steps / (ms / 1e3) / 1e9
+
+    # the same steps one after another on one stream (no overlap), and the per-pass
+    # kernel durations from CUDA events around every launch (a separate timed loop:
+    # the events between launches cost about 10 us a step)
+    serial_steps = max(3, min(args.steps, 500))
+    s1, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    s1.record(stream)
+    for k in range(serial_steps):
+        comp(stream, outs[k % 2], xs[k % 2])
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_serial = s1.elapsed_time(e1) / serial_steps
+    plan.profile(serial_steps)
+    for k in range(serial_steps):
+        comp(stream, outs[k % 2], xs[k % 2])
+    torch.cuda.synchronize(dev)
+    pass_ms, calls = plan.profile_read()
+    plan.profile(0)
+    if dist is not None:
+        t = torch.tensor([ms_serial], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_serial = float(t.item())
 
     # end to end through the public API with pinned host buffers: every step copies
     # its input up, transforms it and copies the result down; consecutive steps are
@@ -361,6 +398,8 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
             "peak_kind": peak_kind,
         },
         "hbm_frac_step": (B_ALG / (ms / args.steps / 1e3) / 1e9) / peak,
+        "ms_per_step_one_stream": ms_serial,
+        "overlap": "consecutive steps alternate between two streams with one compiled plan each",
         "pass_ms": per_launch,
         "passes": [f"{p['note']} L={p['L']} {p['mode']}" for p in passes],
         "gflops": world * FLOP * args.steps / (ms / 1e3) / 1e9,
