@@ -1,4 +1,5 @@
-"""Batched execution (one persistent launch, CUDA-graph replay, plain calls).
+"""Batched execution (one persistent launch, CUDA-graph replay with and without one
+branch per member, plain calls).
 
 Batched results must be bit-identical to the same members run one call at a time with
 the same plan flags: the tile bodies are the same device code with the same
@@ -73,6 +74,22 @@ def test_batch_key_depends_on_members():
     b = N.desc(N.FMT_C64, (1000, 1000), (0, 1))
     assert _desc_key([a, b]) == _desc_key([a, b])
     assert _desc_key([a, b]) != _desc_key([b, a])
+
+
+def test_branch_parallel_graph_is_a_candidate_for_several_members():
+    import torch
+
+    from reikna_b200.batch import MODES, BatchedFFT
+    from reikna_b200.core import ArrayMetadata
+    from reikna_b200.fft import FFT
+
+    assert "graph_par" in MODES
+    dev = torch.device("cuda", 0)  # no plan is compiled in mode "auto" before the first call
+    a = FFT(ArrayMetadata((64, 1024), numpy.complex64), axes=(1,))
+    b = FFT(ArrayMetadata((32, 32), numpy.complex64))
+    modes = [m for m, _ in BatchedFFT([a, b], device=dev).candidates()]
+    assert "graph_par" in modes and "graph" in modes and "persistent" in modes
+    assert "graph_par" not in [m for m, _ in BatchedFFT([a], device=dev).candidates()]
 
 
 # --- GPU ---------------------------------------------------------------------------
