@@ -4,12 +4,12 @@
 Workload (the configuration the headline metric is quoted on): 3-D C2C FFT over all
 axes of a 256 x 256 x 256 complex64 array with a fused output fftshift and 1/N
 scaling transformation.  One step = one forward transform of one array resident in
-HBM; inputs are 134 MB each (larger than the 126 MB L2) and two input/output sets
-alternate between steps.  Consecutive steps are independent and alternate between two
-streams (one compiled plan each), so a step's first pass overlaps the previous step's
-second pass; ``ms_per_step_one_stream`` reports the same steps run back to back on
-one stream, and the roofline's per-kernel durations come from CUDA events around
-every launch in a separate single-stream loop.
+HBM; inputs are 134 MB each (larger than the 126 MB L2) and three input/output sets
+rotate between steps.  Consecutive steps are independent and rotate over three
+streams (one compiled plan and buffer set each), so a step's first pass overlaps the
+earlier steps' second passes; ``ms_per_step_one_stream`` reports the same steps run
+back to back on one stream, and the roofline's per-kernel durations come from CUDA
+events around every launch in a separate single-stream loop.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl own|reference]
 
@@ -45,6 +45,9 @@ ELEM = 8
 ARRAY_BYTES = NTOT * ELEM
 P_MIN = 2
 B_ALG = P_MIN * 2 * ARRAY_BYTES
+# streams the headline loop rotates consecutive steps over (measured per step on one
+# B200: 1 stream 154 us, 2: 134, 3: 120, 4: 124.5)
+LANES = 3
 FLOP = 5 * NTOT * math.log2(NTOT)
 METRIC = "C2C FFT GB/s vs HBM peak, plain vs batched/TC-split at stated err; serve p99 ms"
 CONFIG = {
@@ -54,7 +57,7 @@ CONFIG = {
     "axes": [0, 1, 2],
     "transformations": ["fftshift (output)", "mul_const 1/N (output)"],
     "bytes_per_step_algorithmic": B_ALG,
-    "l2": "inputs larger than L2 (134 MB each), two buffer sets alternate (one per stream)",
+    "l2": "inputs larger than L2 (134 MB each), three buffer sets rotate (one per stream)",
 }
 
 
@@ -229,8 +232,9 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
     gen = torch.Generator(device=dev).manual_seed(1234 + rank)
-    xs = [torch.complex(torch.randn(SHAPE, device=dev, generator=gen), torch.randn(SHAPE, device=dev, generator=gen)) for _ in range(2)]
-    outs = [torch.empty_like(xs[0]) for _ in range(2)]
+    xs = [torch.complex(torch.randn(SHAPE, device=dev, generator=gen), torch.randn(SHAPE, device=dev, generator=gen))
+          for _ in range(LANES)]
+    outs = [torch.empty_like(xs[0]) for _ in range(LANES)]
 
     def build():
         fft = FFT(xs[0])
@@ -240,20 +244,20 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
         fft.parameter.shifted.connect(sc, sc.input, result=sc.output)
         return fft.compile(dev)
 
-    # consecutive steps are independent transforms of alternating buffer sets: step k
-    # runs on stream k % 2 with its own compiled plan (each plan owns the intermediate
-    # between its two passes), so one step's plane pass overlaps the previous step's
-    # lane pass
-    comps = [build(), build()]
+    # consecutive steps are independent transforms of rotating buffer sets: step k runs
+    # on stream k % LANES with its own compiled plan (each plan owns the intermediate
+    # between its two passes), so one step's plane pass overlaps the previous steps'
+    # lane passes
+    comps = [build() for _ in range(LANES)]
     comp = comps[0]
     plan = comp._runner.plan
     launches = plan.launches
     passes = plan.describe()["passes"]
 
     stream = torch.cuda.current_stream(dev)
-    lanes = [torch.cuda.Stream(dev) for _ in range(2)]
+    lanes = [torch.cuda.Stream(dev) for _ in range(LANES)]
     for k in range(args.warmup):
-        comps[k % 2](lanes[k % 2], outs[k % 2], xs[k % 2])
+        comps[k % LANES](lanes[k % LANES], outs[k % LANES], xs[k % LANES])
     torch.cuda.synchronize(dev)
 
     def barrier():
@@ -268,7 +272,7 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
         for s in lanes:
             s.wait_stream(stream)
         for k in range(args.steps):
-            comps[k % 2](lanes[k % 2], outs[k % 2], xs[k % 2])
+            comps[k % LANES](lanes[k % LANES], outs[k % LANES], xs[k % LANES])
         for s in lanes:
             stream.wait_stream(s)
         end.record(stream)
@@ -399,7 +403,7 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
         },
         "hbm_frac_step": (B_ALG / (ms / args.steps / 1e3) / 1e9) / peak,
         "ms_per_step_one_stream": ms_serial,
-        "overlap": "consecutive steps alternate between two streams with one compiled plan each",
+        "overlap": f"consecutive steps rotate over {LANES} streams with one compiled plan and buffer set each",
         "pass_ms": per_launch,
         "passes": [f"{p['note']} L={p['L']} {p['mode']}" for p in passes],
         "gflops": world * FLOP * args.steps / (ms / 1e3) / 1e9,
