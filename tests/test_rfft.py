@@ -329,3 +329,57 @@ def test_half_route_for_real_input(rows, n, dtype, inverse, offset):
     torch.cuda.synchronize()
     assert fft.compile(flags=2**9)._runner.plan.describe()["passes"][0]["note"] != "half"
     assert rel_l2(full.cpu().numpy(), ref) < fft_bound(cdt, n)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,keep", [((2, 3, 512), 257), ((40, 1024), 100), ((7, 64), 5)])
+def test_half_route_batched_and_cropped(shape, keep):
+    """Half-length route through the C-ABI: a real input with any batch dims, and an
+    output keeping fewer than n/2 + 1 bins (its store takes the strided-map path)."""
+    import torch
+
+    from reikna_b200 import _native as N
+
+    rng = numpy.random.default_rng(68)
+    x = rng.standard_normal(shape).astype(numpy.float32)
+    n = shape[-1]
+    d = N.desc(N.FMT_C64, shape, (len(shape) - 1,))
+    d.input = N.edge(N.FMT_F32, shape)
+    d.output = N.edge(N.FMT_C64, shape[:-1] + (keep,))
+    plan = N.Plan(d)
+    assert plan.describe()["passes"][0]["note"] == "half"
+    t = torch.from_numpy(x).cuda()
+    out = torch.zeros(shape[:-1] + (keep,), dtype=torch.complex64, device="cuda")
+    plan.execute([out.data_ptr()], [t.data_ptr()], inverse=0, stream=0)
+    torch.cuda.synchronize()
+    ref = numpy.fft.rfft(x.astype(numpy.float64), axis=-1)[..., :keep]
+    assert rel_l2(out.cpu().numpy(), ref) < fft_bound(numpy.complex64, n)
+
+
+@pytest.mark.gpu
+def test_half_route_transposed_complex_output():
+    """Real frames to a bins-by-frames complex picture: the half-length pass with the
+    lane-fastest store (variant 5) writing complex values."""
+    import torch
+
+    from reikna_b200 import transformations as tr
+    from reikna_b200.core import ArrayMetadata
+    from reikna_b200.fft import FFT
+
+    rng = numpy.random.default_rng(69)
+    frames, n = 300, 256
+    x = rng.standard_normal((frames, n)).astype(numpy.float32)
+    fft = FFT(ArrayMetadata((frames, n), numpy.complex64), axes=(1,))
+    r2c = tr.real_to_complex(ArrayMetadata((frames, n), numpy.float32))
+    fft.parameter.input.connect(r2c, r2c.parameter.output, real=r2c.parameter.input)
+    crop = tr.crop_frequencies(fft.parameter.output)
+    fft.parameter.output.connect(crop, crop.parameter.input, half=crop.parameter.output)
+    tp = tr.transpose_2d(crop.parameter.output)
+    fft.parameter.half.connect(tp, tp.parameter.input, picture=tp.parameter.output)
+    p = fft.describe()["passes"]
+    assert len(p) == 1 and p[0]["note"] == "half" and p[0]["var"] == 5
+    out = torch.empty((n // 2 + 1, frames), dtype=torch.complex64, device="cuda")
+    fft.compile()(None, out, torch.from_numpy(x).cuda())
+    torch.cuda.synchronize()
+    ref = numpy.fft.rfft(x.astype(numpy.float64), axis=1).T
+    assert rel_l2(out.cpu().numpy(), ref) < fft_bound(numpy.complex64, n)
