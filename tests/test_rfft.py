@@ -183,7 +183,7 @@ def test_real_pre_and_antiperiodic_flags_plan_one_pass():
 @pytest.mark.parametrize(
     "shape,dtype",
     [((512,), numpy.float32), ((64, 1024), numpy.float32), ((3, 8192), numpy.float64), ((2, 16), numpy.float32),
-     ((5, 1000), numpy.float32), ((2, 65536), numpy.float32), ((3, 600), numpy.float64)],
+     ((2, 3, 512), numpy.float32), ((5, 1000), numpy.float32), ((2, 65536), numpy.float32), ((3, 600), numpy.float64)],
 )
 def test_aprfft_and_iaprfft(shape, dtype):
     """Against the oracle's restatement of the reference (atol = rtol = 1e-4, the example's
@@ -383,3 +383,37 @@ def test_half_route_transposed_complex_output():
     torch.cuda.synchronize()
     ref = numpy.fft.rfft(x.astype(numpy.float64), axis=1).T
     assert rel_l2(out.cpu().numpy(), ref) < fft_bound(numpy.complex64, n)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("antiperiodic", [False, True])
+def test_real_post_plan_with_output_scale(antiperiodic):
+    """A complex scale on the output edge of a one-pass real transform multiplies every
+    stored bin, the separately stored Nyquist bin included."""
+    import torch
+
+    from reikna_b200 import _native as N
+
+    rng = numpy.random.default_rng(70)
+    rows, n = 9, 512
+    x = rng.standard_normal((rows, n)).astype(numpy.float32)
+    half = n // 2
+    flags = N.FLAG_REAL_POST | (N.FLAG_ANTIPERIODIC if antiperiodic else 0)
+    bins = half if antiperiodic else half + 1
+    d = N.desc(N.FMT_C64, (rows, half), (1,), flags)
+    d.input = N.edge(N.FMT_C64, (rows, half))
+    d.output = N.edge(N.FMT_C64, (rows, bins))
+    d.output.scale_re, d.output.scale_im = 0.5, -0.25
+    plan = N.Plan(d)
+    t = torch.from_numpy(x).cuda()
+    out = torch.zeros((rows, bins), dtype=torch.complex64, device="cuda")
+    plan.execute([out.data_ptr()], [t.data_ptr()], inverse=0, stream=0)
+    torch.cuda.synchronize()
+    if antiperiodic:
+        ref = numpy.fft.rfft(numpy.concatenate([x, -x], axis=1).astype(numpy.float64), axis=1)[:, 1::2]
+    else:
+        ref = numpy.fft.rfft(x.astype(numpy.float64), axis=1)
+    ref = ref * (0.5 - 0.25j)
+    assert rel_l2(out.cpu().numpy(), ref) < fft_bound(numpy.complex64, 2 * n)
+    if not antiperiodic:
+        assert numpy.allclose(out.cpu().numpy()[:, -1], ref[:, -1], atol=1e-3 * numpy.abs(ref).max())
