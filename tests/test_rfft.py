@@ -417,3 +417,39 @@ def test_real_post_plan_with_output_scale(antiperiodic):
     assert rel_l2(out.cpu().numpy(), ref) < fft_bound(numpy.complex64, 2 * n)
     if not antiperiodic:
         assert numpy.allclose(out.cpu().numpy()[:, -1], ref[:, -1], atol=1e-3 * numpy.abs(ref).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("antiperiodic", [False, True])
+def test_real_pre_plan_with_input_scale(antiperiodic):
+    """A complex scale on the input edge of a one-pass inverse real transform acts on the
+    spectrum before the real step (numpy's irfft of the scaled spectrum: the imaginary
+    parts of bins 0 and L are dropped after scaling)."""
+    import torch
+
+    from reikna_b200 import _native as N
+
+    rng = numpy.random.default_rng(71)
+    rows, half = 6, 256
+    c = 0.5 - 0.25j
+    if antiperiodic:
+        f = (rng.standard_normal((rows, half)) + 1j * rng.standard_normal((rows, half))).astype(numpy.complex64)
+        spec = numpy.zeros((rows, 2 * half + 1), numpy.complex128)
+        spec[:, 1::2] = f * c
+        ref = numpy.fft.irfft(spec, axis=1)[:, : 2 * half]
+        bins = half
+    else:
+        f = (rng.standard_normal((rows, half + 1)) + 1j * rng.standard_normal((rows, half + 1))).astype(numpy.complex64)
+        ref = numpy.fft.irfft(f.astype(numpy.complex128) * c, axis=1)
+        bins = half + 1
+    flags = N.FLAG_REAL_PRE | (N.FLAG_ANTIPERIODIC if antiperiodic else 0)
+    d = N.desc(N.FMT_C64, (rows, half), (1,), flags)
+    d.input = N.edge(N.FMT_C64, (rows, bins))
+    d.output = N.edge(N.FMT_C64, (rows, half))
+    d.input.scale_re, d.input.scale_im = c.real, c.imag
+    plan = N.Plan(d)
+    s = torch.from_numpy(f).cuda()
+    out = torch.zeros((rows, 2 * half), dtype=torch.float32, device="cuda")
+    plan.execute([out.data_ptr()], [s.data_ptr()], inverse=1, stream=0)
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), ref) < 2 * fft_bound(numpy.complex64, 2 * half)
