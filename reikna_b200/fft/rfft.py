@@ -13,9 +13,10 @@ As in the reference, the real array is read by a complex FFT of half its length 
 interleaved (re, im) pairs.  When that half length is a power of two (8 to 8192
 points for float32, 4096 for float64) each transform is one pass: the step between
 the real signal's spectrum and the pairs' spectrum runs inside the FFT's last store
-(forward, ``RK_FLAG_REAL_POST``) or first load (inverse, ``RK_FLAG_REAL_PRE``), with
-the antiperiodic twiddles on the other side (``RK_FLAG_ANTIPERIODIC``): one read of
-the input and one write of the output.  Other lengths run the FFT plan between
+(forward: the planner's half-length route for RFFT, which reads any view of the real
+array; ``RK_FLAG_REAL_POST`` for APRFFT) or first load (inverse,
+``RK_FLAG_REAL_PRE``), with the antiperiodic twiddles on the other side
+(``RK_FLAG_ANTIPERIODIC``): one read of the input and one write of the output.  Other lengths run the FFT plan between
 element-wise kernels (``csrc/rk_rfft.cu``).
 """
 
@@ -99,6 +100,29 @@ def _fused_plan(device, batch_shape, half, cdt, flags: int, in_len: int, out_len
         return None
 
 
+def _half_route_plan(device, meta, bins: int):
+    """The planner's half-length route for a real (..., N) input and (..., bins)
+    complex output: the real array is read as sample pairs with scalar loads where a
+    line is not aligned to the pair type, so any view works.  None when N / 2 is not
+    a length that route covers in one pass."""
+    import torch
+
+    cdt = _complex_for(meta.dtype)
+    fmt = N.FMT_C64 if cdt == numpy.complex64 else N.FMT_C128
+    rfmt = N.FMT_F32 if cdt == numpy.complex64 else N.FMT_F64
+    shape = tuple(meta.shape)
+    d = N.desc(fmt, shape, (len(shape) - 1,))
+    d.input = N.edge(rfmt, shape)
+    d.output = N.edge(fmt, shape[:-1] + (bins,))
+    try:
+        if N.describe(d)["passes"][0]["note"] != "half":
+            return None
+        with torch.cuda.device(device):
+            return N.Plan(d)
+    except NotImplementedError:
+        return None
+
+
 def _edges(comp, name):
     leaves = [p.name for p in comp._tr_tree.get_leaf_parameters()]
     if leaves != ["output", "input"]:
@@ -142,9 +166,16 @@ class RFFT(Computation):
         meta = self._meta
         store_last = 0 if self._dont_store_last else 1
         half, cdt = meta.shape[-1] // 2, _complex_for(meta.dtype)
-        fused = _fused_plan(device, meta.shape[:-1], half, cdt, N.FLAG_REAL_POST, half, half + store_last)
-        if fused is not None:
-            return _fused_runner(fused, ann, cdt.itemsize, 0, "input")
+        route = _half_route_plan(device, meta, half + store_last)
+        if route is not None:
+            def run(stream: int, args):
+                out = array_pointer(args["output"], ann["output"])
+                inp = array_pointer(args["input"], ann["input"])
+                route.execute([out], [inp], inverse=0, stream=stream)
+
+            run.launches = route.launches
+            run.plan = route
+            return run
         h = _Half(device, meta.shape[:-1], half, cdt)
 
         def runner(stream: int, args):

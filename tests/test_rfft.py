@@ -453,3 +453,24 @@ def test_real_pre_plan_with_input_scale(antiperiodic):
     plan.execute([out.data_ptr()], [s.data_ptr()], inverse=1, stream=0)
     torch.cuda.synchronize()
     assert rel_l2(out.cpu().numpy(), ref) < 2 * fft_bound(numpy.complex64, 2 * half)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("offset", [0, 1])
+def test_rfft_of_any_view(offset):
+    """RFFT reads the real array through the half-length route's sample-pair loads, so a
+    contiguous view starting on an odd sample works (scalar loads for its lines)."""
+    import torch
+
+    from reikna_b200.fft import RFFT
+
+    rng = numpy.random.default_rng(72)
+    flat = rng.standard_normal(33 * 1024 + offset).astype(numpy.float32)
+    t = torch.from_numpy(flat).cuda()[offset:].view(33, 1024)  # contiguous, odd start for offset 1
+    spec = torch.empty((33, 513), dtype=torch.complex64, device="cuda")
+    c = RFFT(t).compile()
+    assert c.launches == 1
+    c(None, spec, t)
+    torch.cuda.synchronize()
+    ref = numpy.fft.rfft(flat[offset:].reshape(33, 1024).astype(numpy.float64), axis=1)
+    assert rel_l2(spec.cpu().numpy(), ref) < fft_bound(numpy.complex64, 1024)
