@@ -82,58 +82,95 @@ def traffic_from_profiles(kernel_note: str):
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clock and throttle-reason samples taken by a background thread through NVML
+    (read-only queries) every ``period`` seconds while the block runs.  The GPU is
+    found by its PCI bus id, so CUDA_VISIBLE_DEVICES remapping does not matter.
+    ``hold(seconds)`` keeps sampling a little longer (a workload whose timed steps
+    take milliseconds is kept running around them, see ``soak`` in the callers)."""
 
-    QUERY = (
-        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    REASONS = (
+        ("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+        ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+        ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+        ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
     )
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
+    def __init__(self, device_index: int, period: float = 0.01):
+        self.device_index = device_index
+        self.period = period
+        self.rows = []
+        self.error = None
+        self._stop = None
+        self._thread = None
+
+    def _handle(self, nv):
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.device_index)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:  # noqa: BLE001 - fall back to the index
+            return nv.nvmlDeviceGetHandleByIndex(self.device_index)
+
+    def _run(self):
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            try:
+                h = self._handle(nv)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = [(name, getattr(nv, attr, 0)) for name, attr in self.REASONS]
+                while not self._stop.is_set():
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    why = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    util = nv.nvmlDeviceGetUtilizationRates(h).gpu
+                    self.rows.append((sm, mx, why, util, [n for n, bit in bits if why & bit]))
+                    self._stop.wait(self.period)
+            finally:
+                nv.nvmlShutdown()
+        except Exception as e:  # noqa: BLE001 - no NVML: the line says so
+            self.error = f"{type(e).__name__}: {e}"
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE,
-                stderr=subprocess.DEVNULL,
-                text=True,
-            )
-        except FileNotFoundError:
-            self.proc = None
+        import threading
+
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *exc):
-        self.out = ""
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                self.out, _ = self.proc.communicate()
+        self._stop.set()
+        self._thread.join(timeout=5)
 
     def summary(self) -> dict:
-        rows = []
-        for line in (self.out or "").strip().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) >= 9:
-                rows.append(f)
+        rows = list(self.rows)
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0,
+                    "error": self.error}
+        # samples under load: GPU utilisation above zero in NVML's last sampling window
+        busy = [r for r in rows if r[3] > 0] or rows
         return {
-            "sm_mhz": statistics.median(sm) if sm else None,
-            "sm_max_mhz": max(mx) if mx else None,
-            "reasons": reasons,
+            "sm_mhz": statistics.median(r[0] for r in busy),
+            "sm_max_mhz": max(r[1] for r in rows),
+            "reasons": sorted({n for r in busy for n in r[4]}),
             "samples": len(rows),
+            "samples_under_load": len(busy),
+            "source": "NVML, background thread, 10 ms period",
         }
+
+
+def soak(fn, seconds: float) -> None:
+    """Keep the GPU on the workload for ``seconds`` (untimed) so that the clock
+    sampler sees it under load around a short timed region."""
+    import torch
+
+    t_end = time.perf_counter() + seconds
+    while time.perf_counter() < t_end:
+        fn()
+        torch.cuda.synchronize()
 
 
 def cpu_baseline(x_host, seconds: float = 12.0) -> dict:
@@ -264,8 +301,13 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
         if dist is not None:
             dist.barrier()
 
+    def round_of_steps():
+        for k in range(LANES * 8):
+            comps[k % LANES](lanes[k % LANES], outs[k % LANES], xs[k % LANES])
+
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local_rank) as clk:
+        soak(round_of_steps, 0.5)
         barrier()
         torch.cuda.synchronize(dev)
         start.record(stream)
@@ -278,6 +320,7 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
         end.record(stream)
         torch.cuda.synchronize(dev)
         barrier()
+        soak(round_of_steps, 0.2)
     ms = start.elapsed_time(end)
     if dist is not None:
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
@@ -419,10 +462,168 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
         "gpu_launches": launches * args.steps,
         "clocks": clk.summary(),
     }
+    if world == 1 and not args.no_configs:
+        line["configs"] = measure_configs(dev, args)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x_host)
     print(json.dumps(line), flush=True)
     return 0
+
+
+# --- the other configurations, measured beside the headline ----------------------------
+
+
+def _rel(a, b) -> float:
+    import numpy
+
+    a = numpy.asarray(a, numpy.complex128)
+    b = numpy.asarray(b, numpy.complex128)
+    return float(numpy.linalg.norm((a - b).ravel()) / numpy.linalg.norm(b.ravel()))
+
+
+def _events_ms(fn, reps: int) -> float:
+    import torch
+
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s0.record()
+    for _ in range(reps):
+        fn()
+    s1.record()
+    torch.cuda.synchronize()
+    return s0.elapsed_time(s1) / reps
+
+
+def measure_c1(dev, warmup: int) -> dict:
+    """Plain 1-D C2C: 64 x 4096 complex64 along the last axis, forward then inverse.
+    80 buffer sets rotate (160 MB of inputs, more than L2).  Per-call: one forward and
+    one inverse call through the public API per set; graph: the same 160 calls
+    captured once in a CUDA graph and replayed."""
+    import numpy
+    import torch
+
+    from reikna_b200.fft import FFT
+
+    nset, shape = 80, (64, 4096)
+    rng = numpy.random.default_rng(1)
+    x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(numpy.complex64)
+    xs = [torch.from_numpy(x).to(dev) for _ in range(nset)]
+    ys = [torch.empty_like(xs[0]) for _ in range(nset)]
+    zs = [torch.empty_like(xs[0]) for _ in range(nset)]
+    cc = FFT(xs[0], axes=(1,)).compile(dev)
+
+    def pairs():
+        for k in range(nset):
+            cc(None, ys[k], xs[k], 0)
+            cc(None, zs[k], ys[k], 1)
+
+    for _ in range(max(3, warmup)):
+        pairs()
+    t0 = time.perf_counter()
+    ms_calls = _events_ms(pairs, 5) / nset
+    host_us = (time.perf_counter() - t0) / (5 * nset) * 1e6
+    err_f = _rel(ys[0].cpu().numpy(), numpy.fft.fft(x.astype(numpy.complex128), axis=1))
+    err_rt = _rel(zs[0].cpu().numpy(), x)
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        pairs()
+    side.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side):
+        pairs()
+    for _ in range(3):
+        g.replay()
+    ms_graph = _events_ms(g.replay, 10) / nset
+    b_pair = 2 * 2 * x.nbytes            # forward + inverse, each reads and writes the array
+    peak, _ = peaks()
+
+    def entry(ms):
+        gbs = b_pair / (ms / 1e3) / 1e9
+        return {"us_per_pair": ms * 1e3, "gbs": gbs, "hbm_frac": gbs / peak}
+
+    return {
+        "workload": "64x4096 complex64, axis 1, forward + inverse (round trip)",
+        "bytes_algorithmic_per_pair": b_pair,
+        "per_call": dict(entry(ms_calls), host_us_per_pair=host_us),
+        "graph": entry(ms_graph),
+        "rel_l2_vs_fp64": err_f,
+        "round_trip_rel_l2": err_rt,
+        "launches_per_pair": 2 * cc.launches,
+        "l2": f"{nset} buffer sets rotate ({nset * x.nbytes >> 20} MiB of inputs)",
+    }
+
+
+def measure_c2b(dev, warmup: int) -> dict:
+    """3-D FP64 path: 128^3 complex128 over all axes with fused fftshift and 1/N; four
+    buffer sets rotate (134 MB of inputs, more than L2)."""
+    import numpy
+    import torch
+
+    from reikna_b200 import transformations as tr
+    from reikna_b200.fft import FFT
+
+    shape, nset = (128, 128, 128), 4
+    n = 128**3
+    rng = numpy.random.default_rng(3)
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    xs = [torch.from_numpy(x).to(dev) for _ in range(nset)]
+    ys = [torch.empty_like(xs[0]) for _ in range(nset)]
+    fft = FFT(xs[0])
+    sh = tr.fftshift(xs[0])
+    sc = tr.mul_const(xs[0], 1.0 / n)
+    fft.parameter.output.connect(sh, sh.input, shifted=sh.output)
+    fft.parameter.shifted.connect(sc, sc.input, result=sc.output)
+    cc = fft.compile(dev)
+    state = {"k": 0}
+
+    def step():
+        k = state["k"] % nset
+        cc(None, ys[k], xs[k])
+        state["k"] += 1
+
+    for _ in range(max(3, warmup)):
+        step()
+    ms = _events_ms(step, 200)
+    cc(None, ys[0], xs[0])
+    err = _rel(ys[0].cpu().numpy(), numpy.fft.fftshift(numpy.fft.fftn(x)) / n)
+    b_alg = 2 * 2 * x.nbytes              # P_min = 2 (2^21 points, 2^13 complex128 an SM)
+    peak, _ = peaks()
+    gbs = b_alg / (ms / 1e3) / 1e9
+    return {"workload": "128^3 complex128, all axes, fftshift + 1/N (output)", "us_per_step": ms * 1e3,
+            "bytes_algorithmic": b_alg, "gbs": gbs, "hbm_frac": gbs / peak, "rel_l2_vs_fp64": err,
+            "bound": 1e-14 * 21, "passes": [p["note"] for p in cc._runner.plan.describe()["passes"]],
+            "l2": f"{nset} buffer sets rotate"}
+
+
+def measure_configs(dev, args) -> dict:
+    """C1, C2b, C3, C4 and C5 in compact form for the default line (each entry: error
+    against numpy FP64, device time, algorithmic GB/s and fraction of measured HBM)."""
+    import torch
+
+    peak, peak_kind = peaks()
+    out = {"peak_gbs": peak, "peak_kind": peak_kind}
+    t0 = time.perf_counter()
+    steps = max(20, min(args.steps, 200))
+    try:
+        out["C1"] = measure_c1(dev, args.warmup)
+        out["C2b"] = measure_c2b(dev, args.warmup)
+        res, b_alg = measure_batch(dev, steps, args.warmup, modes=("graph_par", "persistent", "auto"))
+        for v in res.values():
+            v["hbm_frac"] = v["gbs"] / peak
+        out["C3"] = {"workload": "batch 1000x3001 (Bluestein) + 1000x1000 + r2c 1000x1000", "bytes_algorithmic": b_alg,
+                     "modes": res, "speedup_vs_plain": res["plain_per_call"]["us"] / res["auto"]["us"]}
+        prec, b_alg = measure_precision(dev, steps, args.warmup)
+        out["C4"] = {"workload": "16384x1024 complex64, axis 1", "bytes_algorithmic": b_alg, "results": prec}
+        torch.cuda.empty_cache()
+        out["C5"] = {
+            "device_data": measure_serve(dev, args.serve_sample, "device", 4, 0.7, clocks=False),
+            "host_data": measure_serve(dev, args.serve_sample, "host", 4, 0.7, clocks=False),
+        }
+    except Exception as e:  # noqa: BLE001 - the headline stands on its own
+        out["error"] = f"{type(e).__name__}: {e}"
+    out["seconds"] = time.perf_counter() - t0
+    return out
 
 
 # --- serving stream ---------------------------------------------------------------
@@ -521,24 +722,22 @@ def _lat_ms(reqs) -> dict:
     return {"p50": float(numpy.percentile(lat, 50)), "p99": float(numpy.percentile(lat, 99)), "mean": float(lat.mean())}
 
 
-def run_serve(args, rank: int, world: int, local_rank: int) -> int:
-    """Serving stream: continuous-batching server against per-call plain execution."""
+def measure_serve(dev, n_requests: int, data: str, streams: int, load: float, clocks: bool = True) -> dict:
+    """The serving stream's first ``n_requests`` requests through the continuous-batching
+    server and through per-call plain execution: a burst (all arrive at t = 0) and a
+    Poisson stream at ``load`` times the served burst rate.  Every result is checked
+    against numpy FP64 on a seeded subset after the timed runs."""
+    import collections
+
     import numpy
     import torch
 
     from reikna_b200.serve import FFTServer, serve_plain
 
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    on_device = args.serve_data == "device"
-    reqs, nbytes = serve_stream(args.requests, 9, dev, on_device)
+    on_device = data == "device"
+    reqs, nbytes = serve_stream(n_requests, 9, dev, on_device)
     total = float(sum(nbytes))
-    srv = FFTServer(dev, memory_budget=40 << 30, streams=args.streams, depth=2)
-    plain_cache = None
-    import collections
-
+    srv = FFTServer(dev, memory_budget=40 << 30, streams=streams, depth=2)
     plain_cache = collections.OrderedDict()
     # warm pass of each arm: plans compiled and resident
     t_prep = time.perf_counter()
@@ -551,21 +750,76 @@ def run_serve(args, rank: int, world: int, local_rank: int) -> int:
     _reset(reqs)
     torch.cuda.synchronize(dev)
     warm_compiles = srv.plans.compiles
-    with Clocks(local_rank) as clk:
+    with Clocks(dev.index) as clk:
         t_srv = srv.run(reqs)
         _reset(reqs)
         t_plain = serve_plain(reqs, dev, cache=plain_cache)
         _reset(reqs)
-        rate = args.load * len(reqs) / t_srv
+        rate = load * len(reqs) / t_srv
         offs = numpy.cumsum(numpy.random.default_rng(10).exponential(1.0 / rate, len(reqs))).tolist()
         t_srv_p = srv.run(reqs, offs)
         lat_srv = _lat_ms(reqs)
         _reset(reqs)
         t_plain_p = serve_plain(reqs, dev, offsets=offs, cache=plain_cache)
         lat_plain = _lat_ms(reqs)
+    # served results against numpy FP64 (a few requests of each kind; outputs of the
+    # stream share pools, so each checked request is served again on its own buffers)
+    errs = {}
+    for r in [r for r in reqs if r.kind == "fft1d"][:2] + [r for r in reqs if r.kind == "fft2d"][:1] + \
+            [r for r in reqs if r.kind == "spectrogram"][:1]:
+        from reikna_b200.serve import FFTRequest
+
+        one = FFTRequest(r.kind, r.data, inverse=r.inverse, nfft=r.nfft, hop=r.hop)
+        srv.run([one])
+        got = one.result.cpu().numpy() if hasattr(one.result, "cpu") else one.result.numpy()
+        x = r.data.cpu().numpy()
+        if r.kind == "fft1d":
+            ref = numpy.fft.fft(x.astype(numpy.complex128), axis=1)
+        elif r.kind == "fft2d":
+            ref = numpy.fft.fft2(x.astype(numpy.complex128))
+        else:
+            nf = got.shape[0]
+            idx = numpy.arange(nf)[:, None] * r.hop + numpy.arange(r.nfft)[None, :]
+            w = 0.5 * (1 - numpy.cos(2 * numpy.pi * numpy.arange(r.nfft) / (r.nfft - 1)))
+            ref = numpy.abs(numpy.fft.rfft(x.astype(numpy.float64)[idx] * w, axis=1))
+        errs[f"{r.kind}{list(r.data.shape)}"] = float(numpy.linalg.norm((got - ref).ravel()) / numpy.linalg.norm(ref.ravel()))
     h2d = sum(r.in_bytes() for r in reqs)
     d2h = sum(int(numpy.prod(r.out_shape())) * (4 if r.kind == "spectrogram" else 8) for r in reqs)
     kinds = collections.Counter(r.kind for r in reqs)
+    return {
+        "requests": len(reqs),
+        "of_stream": "first requests of the seeded 100k-request stream (same generator)",
+        "mix": dict(kinds),
+        "data": data,
+        "streams": streams,
+        "bytes_algorithmic": total,
+        "served": {"s": t_srv, "req_per_s": len(reqs) / t_srv, "gbs": total / t_srv / 1e9},
+        "plain": {"s": t_plain, "req_per_s": len(reqs) / t_plain, "gbs": total / t_plain / 1e9},
+        "speedup_vs_plain": t_plain / t_srv,
+        "poisson": {"rate_req_per_s": rate, "load_vs_served_capacity": load, "served_latency_ms": lat_srv,
+                    "plain_latency_ms": lat_plain, "served_s": t_srv_p, "plain_s": t_plain_p},
+        "groups": srv.groups,
+        "plans": {"prepared": warm_compiles, "prepare_s": t_prep,
+                  "compiled_while_timed": srv.plans.compiles - warm_compiles, "evictions": srv.plans.evictions,
+                  "resident_bytes": srv.plans.bytes, "plain_cache_plans": len(plain_cache)},
+        "h2d_bytes": 0 if on_device else h2d,
+        "d2h_bytes": 0 if on_device else d2h,
+        "rel_l2_vs_fp64": errs,
+        "clocks": clk.summary() if clocks else None,
+    }
+
+
+def run_serve(args, rank: int, world: int, local_rank: int) -> int:
+    """Serving stream: continuous-batching server against per-call plain execution."""
+    import torch
+
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    m = measure_serve(dev, args.requests, args.serve_data, args.streams, args.load)
+    t_srv = m["served"]["s"]
+    total = m["bytes_algorithmic"]
     line = {
         "metric": METRIC,
         "value": total / t_srv / 1e9,
@@ -581,37 +835,25 @@ def run_serve(args, rank: int, world: int, local_rank: int) -> int:
         "data": "synthetic",
         "config": {
             "workload": "serve_stream",
-            "requests": len(reqs),
-            "mix": dict(kinds),
+            "requests": m["requests"],
+            "mix": m["mix"],
             "memory_budget_bytes": 40 << 30,
             "streams": args.streams,
             "data": args.serve_data,
             "note": "value = algorithmic bytes of all requests / wall time of a burst (all arrive at t=0); "
-            + ("inputs and outputs in device memory" if on_device else "host pinned inputs and outputs, copies included"),
+            + ("inputs and outputs in device memory" if args.serve_data == "device"
+               else "host pinned inputs and outputs, copies included"),
         },
-        "req_per_s": len(reqs) / t_srv,
-        "plain": {"value": total / t_plain / 1e9, "req_per_s": len(reqs) / t_plain, "s": t_plain},
-        "speedup_vs_plain": t_plain / t_srv,
-        "poisson": {
-            "rate_req_per_s": rate,
-            "load_vs_served_capacity": args.load,
-            "served_latency_ms": lat_srv,
-            "plain_latency_ms": lat_plain,
-            "served_s": t_srv_p,
-            "plain_s": t_plain_p,
-        },
-        "groups": srv.groups,
-        "plans": {
-            "prepared": warm_compiles,
-            "prepare_s": t_prep,
-            "compiled_while_timed": srv.plans.compiles - warm_compiles,
-            "evictions": srv.plans.evictions,
-            "resident_bytes": srv.plans.bytes,
-            "plain_cache_plans": len(plain_cache),
-        },
-        "e2e": {"value": total / t_srv / 1e9, "unit": "GB/s", "h2d_bytes_per_step": 0 if on_device else h2d,
-                "d2h_bytes_per_step": 0 if on_device else d2h},
-        "clocks": clk.summary(),
+        "req_per_s": m["served"]["req_per_s"],
+        "plain": {"value": m["plain"]["gbs"], "req_per_s": m["plain"]["req_per_s"], "s": m["plain"]["s"]},
+        "speedup_vs_plain": m["speedup_vs_plain"],
+        "poisson": m["poisson"],
+        "groups": m["groups"],
+        "plans": m["plans"],
+        "rel_l2_vs_fp64": m["rel_l2_vs_fp64"],
+        "e2e": {"value": total / t_srv / 1e9, "unit": "GB/s", "h2d_bytes_per_step": m["h2d_bytes"],
+                "d2h_bytes_per_step": m["d2h_bytes"]},
+        "clocks": m["clocks"],
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -648,11 +890,11 @@ def oracle_seconds(shape, axes, sample_rows=None, seconds: float = 4.0):
 # --- batched launch -----------------------------------------------------------------
 
 
-def run_batch(args, rank: int, world: int, local_rank: int) -> int:
+def measure_batch(dev, steps: int, warmup: int, modes=("calls", "graph", "graph_par", "persistent", "auto")):
     """Mixed-size batch: 1000 x 3001 (axis 1, Bluestein), 1000 x 1000 (both axes) and a
     1000 x 1000 float32 real-to-complex transform cropped to 1000 x 501, run as plain
-    per-call execution and as one batch in each mode (calls, CUDA graph, persistent
-    launch, autotuned)."""
+    per-call execution and as one batch in each of ``modes``.  Returns (results by
+    mode, algorithmic bytes per step)."""
     import numpy
     import torch
 
@@ -660,10 +902,6 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> int:
     from reikna_b200.batch import BatchedFFT
     from reikna_b200.fft import FFT
 
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
     rng4, rng5, rng6 = (numpy.random.default_rng(s) for s in (4, 5, 6))
     xa = (rng4.standard_normal((1000, 3001)) + 1j * rng4.standard_normal((1000, 3001))).astype(numpy.complex64)
     xb = (rng5.standard_normal((1000, 1000)) + 1j * rng5.standard_normal((1000, 1000))).astype(numpy.complex64)
@@ -688,7 +926,7 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> int:
     ]
 
     def timed(fn, reps):
-        for _ in range(max(3, args.warmup)):
+        for _ in range(max(3, warmup)):
             fn()
         torch.cuda.synchronize(dev)
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -699,7 +937,7 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> int:
         torch.cuda.synchronize(dev)
         return s0.elapsed_time(s1) / reps
 
-    reps = max(1, min(args.steps, 200))
+    reps = max(1, min(steps, 200))
     singles = [c.compile(dev) for c in comps]
 
     def plain():
@@ -707,7 +945,11 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> int:
             cc(None, o, i)
 
     res = {"plain_per_call": {"us": timed(plain, reps) * 1e3}}
-    for mode in ("calls", "graph", "graph_par", "persistent", "auto"):
+    plain()
+    torch.cuda.synchronize(dev)
+    res["plain_per_call"]["rel_l2_vs_fp64"] = [
+        float(numpy.linalg.norm((o.cpu().numpy() - r).ravel()) / numpy.linalg.norm(r.ravel())) for o, r in zip(outs, refs)]
+    for mode in modes:
         bat = BatchedFFT(comps, device=dev, mode=mode)
         ms = timed(lambda: bat(None, args_list), reps)
         errs = [float(numpy.linalg.norm((o.cpu().numpy() - r).ravel()) / numpy.linalg.norm(r.ravel())) for o, r in zip(outs, refs)]
@@ -720,6 +962,19 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> int:
         bat.close()
     for k, v in res.items():
         v["gbs"] = b_alg / (v["us"] / 1e6) / 1e9
+    return res, b_alg
+
+
+def run_batch(args, rank: int, world: int, local_rank: int) -> int:
+    """The mixed-size batch (``measure_batch``) in every batching mode, autotuned."""
+    import torch
+
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    res, b_alg = measure_batch(dev, args.steps, args.warmup)
+    reps = max(1, min(args.steps, 200))
     best = min((k for k in res if k != "plain_per_call"), key=lambda k: res[k]["us"])
     cpu_s, cpu_threads, samples = 0.0, 1, []
     if not args.no_cpu_baseline:
@@ -756,19 +1011,16 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> int:
 # --- precision mode ---------------------------------------------------------------
 
 
-def run_precision(args, rank: int, world: int, local_rank: int) -> int:
+def measure_precision(dev, steps: int, warmup: int):
     """16384 x 1024 complex64 along the last axis, plain FP32 against the tensor-core
-    split-precision mode, on N(0,1) data and on a 60 dB variant (components +-10^U(-3,0))."""
+    split-precision mode, on N(0,1) data and on a 60 dB variant (components
+    +-10^U(-3,0)).  Returns (results, algorithmic bytes per step)."""
     import numpy
     import torch
 
     from reikna_b200 import _native as N
     from reikna_b200.fft import FFT
 
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
     shape = (16384, 1024)
     nbytes = shape[0] * shape[1] * 8
     b_alg = 2 * nbytes  # P_min = 1
@@ -789,17 +1041,17 @@ def run_precision(args, rank: int, world: int, local_rank: int) -> int:
         for mode, flags in (("fp32", 0), ("split_tc", N.FLAG_SPLIT_TC)):
             comp = FFT(xs[0], axes=(1,)).compile(dev, flags=flags)
             plan = comp._runner.plan
-            for k in range(max(3, args.warmup)):
+            for k in range(max(3, warmup)):
                 comp(None, ys[k % 2], xs[k % 2])
             torch.cuda.synchronize(dev)
-            steps = max(1, min(args.steps, 500))
+            nsteps = max(1, min(steps, 500))
             s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s0.record()
-            for k in range(steps):
+            for k in range(nsteps):
                 comp(None, ys[k % 2], xs[k % 2])
             s1.record()
             torch.cuda.synchronize(dev)
-            ms = s0.elapsed_time(s1) / steps
+            ms = s0.elapsed_time(s1) / nsteps
             comp(None, ys[0], xs[0])
             y = ys[0].cpu().numpy()
             err = float(numpy.linalg.norm((y - ref).ravel()) / numpy.linalg.norm(ref.ravel()))
@@ -812,6 +1064,20 @@ def run_precision(args, rank: int, world: int, local_rank: int) -> int:
                 "kernel": plan.describe()["passes"][0]["note"],
             }
         out[label] = res
+    return out, b_alg
+
+
+def run_precision(args, rank: int, world: int, local_rank: int) -> int:
+    """FP32 against the tensor-core split mode (``measure_precision``)."""
+    import torch
+
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    shape = (16384, 1024)
+    peak, peak_kind = peaks()
+    out, b_alg = measure_precision(dev, args.steps, args.warmup)
     cpu = None
     if not args.no_cpu_baseline:
         t, threads, desc = oracle_seconds(shape, (1,), 1024)
@@ -991,6 +1257,10 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["own", "reference"], default="own")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="fft3d: skip the compact C1/C2b/C3/C4/C5 measurements after the headline")
+    ap.add_argument("--serve-sample", type=int, default=300,
+                    help="fft3d: requests of the serving stream measured in the configs object")
     ap.add_argument("--workload", choices=["fft3d", "serve", "precision", "batch", "next"], default="fft3d",
                     help="fft3d: the headline 256^3 transform; serve: the request stream; "
                     "precision: FP32 against the tensor-core split mode on 16384 x 1024; "

@@ -256,7 +256,8 @@ RK_API int rk_iaprfft_pre(void* z, const void* x, const void* table, int32_t fmt
  * may overlap on the GPU race.  The first call on a device resolves the static
  * arrays and fills its twiddle tables (kernel launches plus a device
  * synchronisation): make it before any stream capture.  Larger sizes are rejected
- * with RK_ERR_INVALID.
+ * with RK_ERR_INVALID, and so are a stream or arrays that do not belong to the
+ * current device (the static arrays used are the current device's).
  */
 RK_API int rk_fft1d_c64_noalloc(void* out, const void* in, int64_t n, int64_t batch, int32_t inverse, void* stream);
 
@@ -291,6 +292,28 @@ RK_API const char* rk_version(void);
 /* Device status word of the current device (nonzero: a kernel gave up a bounded
  * wait, RK_ERR_DEVICE territory).  Synchronises the device; clear = 1 resets it. */
 RK_API int rk_device_status(int32_t* status, int32_t clear);
+
+/* Status bits of the device status word. */
+#define RK_STATUS_TIMEOUT 1      /* a bounded wait (copy, cluster exchange, batch or pair
+                                    dependency) ran out of its limit */
+#define RK_STATUS_BAD_VARIANT 2  /* a batched task had no compiled tile body */
+
+/* Limit, in SM clock cycles, of every bounded wait in the library's kernels on the
+ * current device (default 2e9, about one second).  No counterpart in the reference
+ * (reikna's kernels never wait on each other).  Set / read. */
+RK_API int rk_set_wait_limit(int64_t cycles);
+RK_API int rk_get_wait_limit(int64_t* cycles);
+
+/* Synchronise `stream` and return RK_ERR_DEVICE (with the word in rk_last_error) if
+ * the current device's status word is nonzero; the word is left as it is. */
+RK_API int rk_stream_check(void* stream);
+
+/* Self-test of the bounded waits: one persistent-batch task whose dependency can never
+ * complete (the pass it waits for has no tiles), run on `stream` and synchronised.
+ * The wait gives up after the current wait limit, the task's body is skipped, and the
+ * call returns RK_ERR_DEVICE with RK_STATUS_TIMEOUT set in the status word (clear it
+ * with rk_device_status(&w, 1) afterwards).  No counterpart in the reference. */
+RK_API int rk_selftest_stalled_wait(void* stream);
 
 /* sizeof(rk_edge) and sizeof(rk_fft_desc) as compiled, for binding checks. */
 RK_API int rk_abi_sizes(int64_t* edge_bytes, int64_t* desc_bytes);

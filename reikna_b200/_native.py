@@ -61,6 +61,10 @@ EXPORTED = (
     "rk_fft_profile",
     "rk_fft_profile_read",
     "rk_device_status",
+    "rk_set_wait_limit",
+    "rk_get_wait_limit",
+    "rk_stream_check",
+    "rk_selftest_stalled_wait",
     "rk_fft1d_c64_noalloc",
     "rk_batch_create",
     "rk_batch_execute",
@@ -198,6 +202,10 @@ def lib() -> ctypes.CDLL:
         L.rk_abi_sizes.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
         L.rk_fft_profile.argtypes = [vp, ctypes.c_int32]
         L.rk_device_status.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
+        L.rk_set_wait_limit.argtypes = [ctypes.c_int64]
+        L.rk_get_wait_limit.argtypes = [ctypes.POINTER(ctypes.c_int64)]
+        L.rk_stream_check.argtypes = [vp]
+        L.rk_selftest_stalled_wait.argtypes = [vp]
         L.rk_fft1d_c64_noalloc.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, vp]
         L.rk_fft_profile_read.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
         i32p, i64p = ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)
@@ -333,6 +341,27 @@ def device_status(clear: bool = False) -> int:
     v = ctypes.c_int32(0)
     check(lib().rk_device_status(ctypes.byref(v), int(bool(clear))))
     return int(v.value)
+
+
+STATUS_TIMEOUT = 1
+STATUS_BAD_VARIANT = 2
+
+
+def set_wait_limit(cycles: int) -> None:
+    """Limit, in SM clock cycles, of the kernels' bounded waits on the current device."""
+    check(lib().rk_set_wait_limit(int(cycles)))
+
+
+def wait_limit() -> int:
+    v = ctypes.c_int64(0)
+    check(lib().rk_get_wait_limit(ctypes.byref(v)))
+    return int(v.value)
+
+
+def stream_check(stream: int = 0) -> None:
+    """Synchronise ``stream``; raise :class:`NativeError` (``ERR_DEVICE``) if the device
+    status word is set (a bounded wait ran out)."""
+    check(lib().rk_stream_check(ctypes.c_void_p(stream)))
 
 
 class Batch:

@@ -130,12 +130,15 @@ class _Variant:
         import torch
 
         key = tuple((tuple(o), tuple(i), inv, tuple(complex(s) for s in sc)) for o, i, inv, sc in calls)
+        ext = torch.cuda.ExternalStream(stream) if stream else torch.cuda.current_stream()
         g = self._graphs.get(key)
         if g is None:
             if len(self._graphs) >= 8:
                 self._graphs.clear()
             side = torch.cuda.Stream()
-            side.wait_stream(torch.cuda.current_stream())
+            # the eager run and the capture come after the caller's pending work on
+            # its stream (which may still be writing the inputs or reading the outputs)
+            side.wait_stream(ext)
             # one eager run first: per-call host state (tensor maps, staging) is settled
             # before capture
             with torch.cuda.stream(side):
@@ -145,7 +148,6 @@ class _Variant:
             with torch.cuda.graph(g, stream=side):
                 self._launch_calls(calls, side.cuda_stream)
             self._graphs[key] = g
-        ext = torch.cuda.ExternalStream(stream) if stream else torch.cuda.current_stream()
         with torch.cuda.stream(ext):
             g.replay()
 

@@ -1,17 +1,20 @@
 // Asynchronous bulk copies (TMA) and mbarriers for sm_100a, in inline PTX.
 //
-// Waits are bounded: a wait that does not complete within RK_WAIT_LIMIT polls sets
-// bit RK_STATUS_TIMEOUT in the device status word and returns false, so a kernel
-// never spins forever (the host reads the word with rk_device_status()).
+// Waits are bounded: a wait that does not complete within RK_WAIT_LIMIT polls, or
+// within the wait limit in SM clock cycles (about one second unless the host sets
+// another with rk_set_wait_limit), sets bit RK_STATUS_TIMEOUT in the device status
+// word and returns false, so a kernel never spins forever (the host reads the word
+// with rk_device_status()).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "rk_params.h"
+
 namespace rk {
 
 constexpr uint32_t RK_WAIT_LIMIT = 1u << 26;
-constexpr int32_t RK_STATUS_TIMEOUT = 1;
-constexpr int32_t RK_STATUS_BAD_VARIANT = 2;   // batched task with no compiled tile body
+// status bits RK_STATUS_TIMEOUT / RK_STATUS_BAD_VARIANT: include/reikna_b200.h
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -53,13 +56,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // about one second of SM clock: no legitimate wait in these kernels comes near it
 constexpr long long RK_WAIT_CYCLES = 2000000000LL;
 
+// The device status block is four 32-bit words: [0] status bits, [1] unused,
+// [2..3] the wait limit in SM clock cycles (int64, set by rk_set_wait_limit).
+// Without a status block the default limit applies.
+__device__ __forceinline__ long long wait_limit(const int32_t* status) {
+    return status ? *reinterpret_cast<const volatile long long*>(status + 2) : RK_WAIT_CYCLES;
+}
+
 // bounded wait on phase `parity`; false (and the status bit set) on timeout
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* status) {
     if (mbar_try_wait(bar, parity)) return true;
-    const long long t0 = clock64();
+    const long long t0 = clock64(), lim = wait_limit(status);
     for (uint32_t i = 0; i < RK_WAIT_LIMIT; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (clock64() - t0 > RK_WAIT_CYCLES) break;
+        if (clock64() - t0 > lim) break;
     }
     if (status) atomicOr(status, RK_STATUS_TIMEOUT);
     return false;
@@ -82,10 +92,10 @@ __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t pa
 
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, int32_t* status) {
     if (mbar_try_wait_cluster(bar, parity)) return true;
-    const long long t0 = clock64();
+    const long long t0 = clock64(), lim = wait_limit(status);
     for (uint32_t i = 0; i < RK_WAIT_LIMIT; ++i) {
         if (mbar_try_wait_cluster(bar, parity)) return true;
-        if (clock64() - t0 > RK_WAIT_CYCLES) break;
+        if (clock64() - t0 > lim) break;
     }
     if (status) atomicOr(status, RK_STATUS_TIMEOUT);
     return false;

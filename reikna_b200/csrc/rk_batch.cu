@@ -135,9 +135,12 @@ __global__ void __launch_bounds__(BATCH_NT, 2) k_batch(const BatchArgs a) {
     extern __shared__ __align__(16) unsigned char rk_smem[];
     __shared__ __align__(16) PassParams s_prm;
     __shared__ long long s_task[2];
+    __shared__ int s_healthy;
     static_assert(sizeof(PassParams) % 16 == 0, "parameter copy moves 16-byte words");
-    bool healthy = true;
-    if (threadIdx.x == 0) s_task[0] = (long long)atomicAdd(a.next, 1ull);
+    if (threadIdx.x == 0) {
+        s_task[0] = (long long)atomicAdd(a.next, 1ull);
+        s_healthy = 1;
+    }
     __syncthreads();
     for (int cur = 0;; cur ^= 1) {
         const long long t = s_task[cur];
@@ -153,19 +156,21 @@ __global__ void __launch_bounds__(BATCH_NT, 2) k_batch(const BatchArgs a) {
         if (dep >= 0 && threadIdx.x == 0) {
             const unsigned long long need = (unsigned long long)a.passes[dep].nblocks;
             bool ok = ld_acquire(a.done + dep) >= need;
-            if (!ok && healthy) {
-                const long long t0 = clock64();
+            if (!ok && s_healthy) {
+                const long long t0 = clock64(), lim = wait_limit(a.status);
                 while (!(ok = ld_acquire(a.done + dep) >= need))
-                    if (clock64() - t0 > RK_WAIT_CYCLES) break;
+                    if (clock64() - t0 > lim) break;
             }
             if (!ok) {
-                healthy = false;
+                s_healthy = 0;
                 atomicOr(a.status, RK_STATUS_TIMEOUT);
             }
         }
         __syncthreads();
         if (dep >= 0) __threadfence();
-        if (!batch_dispatch(bp->variant, &s_prm, tk.block, rk_smem) && threadIdx.x == 0)
+        // after a wait ran out the CTA's results are void (the status word says so):
+        // it only marks its remaining tasks done, so nothing else waits on them
+        if (s_healthy && !batch_dispatch(bp->variant, &s_prm, tk.block, rk_smem) && threadIdx.x == 0)
             atomicOr(a.status, RK_STATUS_BAD_VARIANT);
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -370,4 +375,53 @@ extern "C" int rk_batch_info(const rk_batch* b, int64_t* ntasks, int32_t* npasse
     if (npasses) *npasses = (int32_t)b->passes.size();
     if (grid) *grid = b->grid;
     return RK_OK;
+}
+
+extern "C" int rk_selftest_stalled_wait(void* stream) {
+    using namespace rk;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    DeviceTables* tabs = nullptr;
+    int rc = e == cudaSuccess ? device_tables(dev, &tabs) : RK_ERR_CUDA;
+    if (rc) {
+        set_error(std::string("rk_selftest_stalled_wait: ") + cudaGetErrorString(e));
+        return rc;
+    }
+    // pass 0: one tile and no task, so it never completes; pass 1: one task that
+    // depends on it (no tile body: the variant id matches none)
+    BatchPass hp[2];
+    memset(hp, 0, sizeof(hp));
+    hp[0].nblocks = 1;
+    hp[0].variant = -1;
+    hp[0].dep = -1;
+    hp[1].nblocks = 1;
+    hp[1].variant = -1;
+    hp[1].dep = 0;
+    BatchTask ht = {1, 0, 0};
+    void* mem = nullptr;
+    const size_t pbytes = sizeof(hp), tbytes = sizeof(ht), cbytes = 3 * sizeof(unsigned long long);
+    const size_t toff = (pbytes + 255) / 256 * 256, coff = toff + 256;
+    cudaStream_t st = (cudaStream_t)stream;
+    e = cudaMalloc(&mem, coff + cbytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(mem, hp, pbytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync((char*)mem + toff, &ht, tbytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync((char*)mem + coff, 0, cbytes, st);
+    if (e == cudaSuccess) {
+        BatchArgs a;
+        a.passes = reinterpret_cast<const BatchPass*>(mem);
+        a.tasks = reinterpret_cast<const BatchTask*>((char*)mem + toff);
+        a.ntasks = 1;
+        a.next = reinterpret_cast<unsigned long long*>((char*)mem + coff);
+        a.done = a.next + 1;
+        a.status = tabs->status;
+        k_batch<<<1, BATCH_NT, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (mem) cudaFree(mem);
+    if (e != cudaSuccess) {
+        set_error(std::string("rk_selftest_stalled_wait: ") + cudaGetErrorString(e));
+        return RK_ERR_CUDA;
+    }
+    return rk_stream_check(stream);
 }

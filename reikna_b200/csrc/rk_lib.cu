@@ -26,6 +26,7 @@
 #include <string>
 #include <vector>
 
+#include "rk_async.cuh"
 #include "rk_internal.h"
 #include "rk_kernels.cuh"
 
@@ -123,8 +124,14 @@ int device_tables(int device, DeviceTables** out) {
     CK(cudaMalloc(&t->tw4lo_f, TW4_HALF * sizeof(float2)));
     CK(cudaMalloc(&t->tw4hi_d, TW4_HALF * sizeof(double2)));
     CK(cudaMalloc(&t->tw4lo_d, TW4_HALF * sizeof(double2)));
-    CK(cudaMalloc(&t->status, sizeof(int32_t)));
-    CK(cudaMemset(t->status, 0, sizeof(int32_t)));
+    // status block: [0] status bits, [1] unused, [2..3] wait limit (SM clock cycles)
+    CK(cudaMalloc(&t->status, 4 * sizeof(int32_t)));
+    {
+        int32_t init[4] = {0, 0, 0, 0};
+        const long long lim = RK_WAIT_CYCLES;
+        memcpy(init + 2, &lim, sizeof(lim));
+        CK(cudaMemcpy(t->status, init, sizeof(init), cudaMemcpyHostToDevice));
+    }
     t->bytes = nf * 8 + ndd * 16 + TW4_HALF * 48;
     for (const StageSeg& s : sf) {
         const int n = (s.R - 1) * s.J;
@@ -895,6 +902,55 @@ int rk_device_status(int32_t* status, int32_t clear) {
     CK(cudaDeviceSynchronize());
     CK(cudaMemcpy(status, t->status, sizeof(int32_t), cudaMemcpyDeviceToHost));
     if (clear) CK(cudaMemset(t->status, 0, sizeof(int32_t)));
+    return RK_OK;
+}
+
+int rk_set_wait_limit(int64_t cycles) {
+    if (cycles < 1000) {
+        set_error("rk_set_wait_limit: the limit must be at least 1000 SM clock cycles");
+        return RK_ERR_INVALID;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    DeviceTables* t = nullptr;
+    int rc = device_tables(dev, &t);
+    if (rc) return rc;
+    const long long lim = cycles;
+    CK(cudaMemcpy(t->status + 2, &lim, sizeof(lim), cudaMemcpyHostToDevice));
+    return RK_OK;
+}
+
+int rk_get_wait_limit(int64_t* cycles) {
+    if (!cycles) {
+        set_error("null argument");
+        return RK_ERR_INVALID;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    DeviceTables* t = nullptr;
+    int rc = device_tables(dev, &t);
+    if (rc) return rc;
+    long long lim = 0;
+    CK(cudaMemcpy(&lim, t->status + 2, sizeof(lim), cudaMemcpyDeviceToHost));
+    *cycles = lim;
+    return RK_OK;
+}
+
+int rk_stream_check(void* stream) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    DeviceTables* t = nullptr;
+    int rc = device_tables(dev, &t);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize((cudaStream_t)stream));
+    int32_t v = 0;
+    CK(cudaMemcpy(&v, t->status, sizeof(v), cudaMemcpyDeviceToHost));
+    if (v) {
+        set_error("device status word " + std::to_string(v) +
+                  ((v & RK_STATUS_TIMEOUT) ? " (a bounded wait ran out)" : "") +
+                  ((v & RK_STATUS_BAD_VARIANT) ? " (a batched task had no tile body)" : ""));
+        return RK_ERR_DEVICE;
+    }
     return RK_OK;
 }
 

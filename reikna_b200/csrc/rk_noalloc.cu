@@ -14,7 +14,8 @@
 // Limits and sharing: batch * n <= RK_NOALLOC_MAX_ELEMS complex64 elements (the
 // scratch is 32 MiB per device that loads the library).  Every call on a device uses
 // the same scratch, so calls that can overlap on the GPU (different streams, no
-// ordering between them) race; calls on one stream are ordered and safe.  The first
+// ordering between them) race; calls on one stream are ordered and safe.  The
+// current device must own the stream and both arrays (checked).  The first
 // call on each device resolves the arrays' device addresses with
 // cudaGetSymbolAddress and fills the twiddle tables with a few kernel launches and a
 // device synchronisation; make that first call before any stream capture.  Pass A
@@ -166,6 +167,33 @@ extern "C" int rk_fft1d_c64_noalloc(void* out, const void* in, int64_t n, int64_
     if (e != cudaSuccess) {
         set_error(std::string("rk_fft1d_c64_noalloc: ") + cudaGetErrorString(e));
         return RK_ERR_CUDA;
+    }
+    // the static arrays used below are the current device's: the stream and both
+    // arrays must belong to that device too
+    if (stream) {
+        int sdev = -1;
+        e = cudaStreamGetDevice((cudaStream_t)stream, &sdev);
+        if (e != cudaSuccess) {
+            set_error(std::string("rk_fft1d_c64_noalloc: stream: ") + cudaGetErrorString(e));
+            return RK_ERR_INVALID;
+        }
+        if (sdev != dev) {
+            set_error("rk_fft1d_c64_noalloc: the stream belongs to device " + std::to_string(sdev) +
+                      ", not to the current device " + std::to_string(dev));
+            return RK_ERR_INVALID;
+        }
+    }
+    const void* arrays[2] = {out, in};
+    for (int i = 0; i < 2; ++i) {
+        cudaPointerAttributes pa;
+        e = cudaPointerGetAttributes(&pa, arrays[i]);
+        if (e != cudaSuccess || (pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) ||
+            pa.device != dev) {
+            cudaGetLastError();
+            set_error(std::string("rk_fft1d_c64_noalloc: ") + (i ? "in" : "out") +
+                      " must be device memory of the current device " + std::to_string(dev));
+            return RK_ERR_INVALID;
+        }
     }
     NaDevice* d = nullptr;
     int rc = na_setup(dev, &d);

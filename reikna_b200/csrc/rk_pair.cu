@@ -74,9 +74,9 @@ __global__ void __launch_bounds__(PairCfg<T, LR, LC>::NT, 3) k_pair(const __grid
                 const unsigned int need = (unsigned int)a.a_per_plane;
                 bool ok = ld_acquire_u32(a.rows_done + plane) >= need;
                 if (!ok && healthy) {
-                    const long long t0 = clock64();
+                    const long long t0 = clock64(), lim = wait_limit(a.status);
                     while (!(ok = ld_acquire_u32(a.rows_done + plane) >= need))
-                        if (clock64() - t0 > RK_WAIT_CYCLES) break;
+                        if (clock64() - t0 > lim) break;
                 }
                 if (!ok) {
                     healthy = false;

@@ -30,7 +30,17 @@ they arrive and keeps the GPU busy with them:
 
 Inputs are host tensors (pinned ones make the copies asynchronous); results come back
 in pinned host tensors the server allocates.  In-place transforms keep one staging
-buffer per group.
+buffer per group.  Device tensors are accepted too: the server orders its work after
+the submitter's stream as it was at :meth:`FFTServer.submit` (an event recorded there)
+and keeps the tensors alive for its own streams (``record_stream``); a consumer of a
+device result waits on the request's ``event``.
+
+**Failures** stay with the requests they belong to.  A request whose staging alone
+exceeds ``memory_budget`` is rejected at submission (``status == "rejected"``); a
+waiting request can be cancelled (:meth:`FFTServer.cancel`); a group whose plan cannot
+be compiled, or whose buffers cannot be allocated, or whose launch raises, ends with
+``status == "failed"`` and the exception in ``error``, while every other group carries
+on.  ``done`` is set for every final status.
 """
 
 from __future__ import annotations
@@ -78,6 +88,10 @@ class FFTRequest:
     launched: float = 0.0
     finished: float = 0.0
     done: bool = False
+    status: str = "new"     # waiting, running, done, failed, cancelled, rejected
+    error: object = None    # the exception of a failed or rejected request
+    ready: object = None    # event on the submitter's stream (device inputs / outputs)
+    event: object = None    # completion event of the request's group on the GPU
 
     def key(self):
         shape = tuple(self.data.shape)
@@ -106,9 +120,16 @@ class FFTRequest:
             return (_frames(self.data.shape[0], self.nfft, self.hop), self.nfft // 2 + 1)
         return tuple(self.data.shape)
 
+    def on_device(self) -> bool:
+        return bool(getattr(self.data, "is_cuda", False) or getattr(self.out, "is_cuda", False))
+
     @property
     def latency(self) -> float:
         return self.finished - self.arrival
+
+
+class AdmissionError(MemoryError):
+    """A request needs more staging memory than the server's whole budget."""
 
 
 def _computation(key, rows: int):
@@ -170,6 +191,7 @@ class _Group:
     bytes: int
     event: object = None
     buffers: list = field(default_factory=list)
+    error: object = None
 
 
 class FFTServer:
@@ -193,10 +215,9 @@ class FFTServer:
         self.memory_budget = int(memory_budget)
         self.depth = int(depth)
         self.max_group_bytes = int(max_group_bytes)
-        with torch.cuda.device(self.device):
-            self.streams = [torch.cuda.Stream(self.device) for _ in range(streams)]
-            self.upload = torch.cuda.Stream(self.device)
-            self.download = torch.cuda.Stream(self.device)
+        self.nstreams = int(streams)
+        self.streams = None          # created with the first launch
+        self.upload = self.download = None
         self.plans = PlanCache(self.device, plan_budget)
         self._class_stream = {}
         self._waiting = collections.OrderedDict()  # class key -> deque of requests
@@ -204,13 +225,56 @@ class FFTServer:
         self._staged = 0
         self.groups = 0
         self.completed = 0
+        self.failed = 0
+        self.rejected = 0
+        self.cancelled = 0
+
+    def _streams(self):
+        import torch
+
+        if self.streams is None:
+            with torch.cuda.device(self.device):
+                self.streams = [torch.cuda.Stream(self.device) for _ in range(self.nstreams)]
+                self.upload = torch.cuda.Stream(self.device)
+                self.download = torch.cuda.Stream(self.device)
+        return self.streams
 
     # -- intake ------------------------------------------------------------------
     def submit(self, req: FFTRequest, now: float | None = None) -> FFTRequest:
+        """Queue ``req``.  A request whose staging alone is larger than the whole
+        memory budget can never be admitted: it comes back with ``status ==
+        "rejected"`` and an :class:`AdmissionError`.  For device inputs or outputs an
+        event is recorded on the submitter's current stream; the server's work on the
+        request waits for it."""
         key = req.key()
         req.arrival = time.perf_counter() if now is None else now
+        if not self._direct([req]) and self.group_bytes([req]) > self.memory_budget:
+            req.status, req.done, req.finished = "rejected", True, req.arrival
+            req.error = AdmissionError(
+                f"request stages {self.group_bytes([req])} bytes, over the {self.memory_budget}-byte budget")
+            self.rejected += 1
+            return req
+        if req.on_device():
+            import torch
+
+            req.ready = torch.cuda.Event()
+            req.ready.record(torch.cuda.current_stream(self.device))
+        req.status = "waiting"
         self._waiting.setdefault(key, collections.deque()).append(req)
         return req
+
+    def cancel(self, req: FFTRequest) -> bool:
+        """Withdraw a request that is still waiting; True if it was.  A request already
+        on the GPU runs to the end (its group shares buffers and launches)."""
+        if req.status != "waiting":
+            return False
+        q = self._waiting.get(req.key())
+        if q is None or req not in q:
+            return False
+        q.remove(req)
+        req.status, req.done, req.finished = "cancelled", True, time.perf_counter()
+        self.cancelled += 1
+        return True
 
     @property
     def pending(self) -> int:
@@ -222,7 +286,7 @@ class FFTServer:
     def stream_of(self, key) -> int:
         s = self._class_stream.get(key)
         if s is None:
-            s = self._class_stream[key] = len(self._class_stream) % len(self.streams)
+            s = self._class_stream[key] = len(self._class_stream) % self.nstreams
         return s
 
     def _next_class(self):
@@ -260,6 +324,11 @@ class FFTServer:
                 b += int(numpy.prod(r.out_shape())) * 4
         return b
 
+    @staticmethod
+    def _direct(reqs) -> bool:
+        """Device inputs with device outputs: transformed in place of staging."""
+        return all(getattr(r.data, "is_cuda", False) and getattr(r.out, "is_cuda", False) for r in reqs)
+
     def _take(self, key):
         q = self._waiting[key]
         take = [q.popleft()]
@@ -271,7 +340,7 @@ class FFTServer:
 
     def step(self) -> int:
         """Retire finished groups, then launch groups while streams and memory allow.
-        Returns the number of groups launched."""
+        Returns the number of groups launched (failed ones included)."""
         self._retire()
         launched = 0
         while True:
@@ -280,7 +349,7 @@ class FFTServer:
                 break
             s = self.stream_of(key)
             reqs = self._take(key)
-            need = self.group_bytes(reqs)
+            need = 0 if self._direct(reqs) else self.group_bytes(reqs)
             if self._staged and self._staged + need > self.memory_budget:
                 # wait for memory: put the requests back at the head of their queue
                 self._waiting[key].extendleft(reversed(reqs))
@@ -289,106 +358,171 @@ class FFTServer:
             launched += 1
         return launched
 
+    # allocation of staging buffers (a separate method so that it can be replaced)
+    def _alloc(self, shape, dtype):
+        import torch
+
+        return torch.empty(shape, dtype=dtype, device=self.device)
+
+    def _plans_for(self, key, reqs):
+        """Every compiled plan the group needs, before any of its work is queued, so
+        that a compile or allocation failure leaves nothing in flight."""
+        if key[0] == "spectrogram" or self._direct(reqs) and key[0] == "fft2d":
+            return {1: self.plans.get(key, 1)}
+        sizes = set()
+        if self._direct(reqs):
+            for r in reqs:
+                sizes.update(binary_pieces(r.rows()))
+        else:
+            sizes.update(binary_pieces(sum(r.rows() for r in reqs)))
+        return {k: self.plans.get(key, k) for k in sorted(sizes)}
+
+    def _fail(self, reqs, err) -> None:
+        now = time.perf_counter()
+        for r in reqs:
+            r.status, r.error, r.done, r.finished = "failed", err, True, now
+        self.failed += len(reqs)
+
     def _launch(self, key, reqs, s: int, need: int) -> None:
         """Three-stage pipeline of one group: host-to-device copies on the upload
         stream, the transforms on the class's compute stream, device-to-host copies on
         the download stream, chained by events.  Uploads of later groups run while
-        earlier groups compute and download (the link carries both directions at once)."""
+        earlier groups compute and download (the link carries both directions at once).
+        A failure before anything is queued fails the group's requests only; one after
+        (a launch that raises) also waits for the group's queued work before its
+        buffers are released."""
         import torch
 
-        stream = self.streams[s]
+        try:
+            plans = self._plans_for(key, reqs)
+        except Exception as e:  # noqa: BLE001 - a failure stays with its group
+            self._fail(reqs, e)
+            return
+        streams = self._streams()
+        stream = streams[s]
         now = time.perf_counter()
         g = _Group(key, reqs, s, need)
-        spec = key[0] == "spectrogram"
-        if all(r.data.is_cuda and r.out is not None and r.out.is_cuda for r in reqs):
-            # device-resident requests with device outputs: no staging, each request
-            # is transformed from its input straight into its output
-            g.bytes = 0
+        for r in reqs:
+            r.launched, r.status = now, "running"
+        try:
             with torch.cuda.device(self.device):
-                for r in reqs:
-                    if spec:
-                        self.plans.get(key, 1)(stream, r.out, r.data)
-                    elif key[0] == "fft2d":
-                        self.plans.get(key, 1)(stream, r.out[None], r.data[None], key[-1])
-                    else:
-                        off = 0
-                        for piece in binary_pieces(r.rows()):
-                            self.plans.get(key, piece)(stream, r.out[off : off + piece], r.data[off : off + piece], key[-1])
-                            off += piece
-                    r.result = r.out
-                g.event = torch.cuda.Event()
-                g.event.record(stream)
-            for r in reqs:
-                r.launched = now
-            self._inflight[s].append(g)
-            self.groups += 1
-            return
-        with torch.cuda.device(self.device):
-            with torch.cuda.stream(self.upload):
-                if spec:
-                    fr, bins = reqs[0].out_shape()
-                    src = torch.empty((len(reqs), key[1]), dtype=torch.float32, device=self.device)
-                    dst = torch.empty((len(reqs), fr, bins), dtype=torch.float32, device=self.device)
-                    for i, r in enumerate(reqs):
-                        src[i].copy_(r.data, non_blocking=True)
-                    g.buffers = [src, dst]
+                if self._direct(reqs):
+                    g.bytes = 0
+                    self._run_direct(key, reqs, plans, stream, g)
                 else:
-                    rows = sum(r.rows() for r in reqs)
-                    shape = (rows, key[1]) if key[0] == "fft1d" else (rows, key[1], key[2])
-                    src = dst = torch.empty(shape, dtype=torch.complex64, device=self.device)
-                    off = 0
-                    for r in reqs:
-                        n = r.rows()
-                        (src[off : off + n] if key[0] == "fft1d" else src[off]).copy_(r.data, non_blocking=True)
-                        off += n
-                    g.buffers = [src]
-                uploaded = torch.cuda.Event()
-                uploaded.record(self.upload)
-            stream.wait_event(uploaded)
-            if spec:
-                cc = self.plans.get(key, 1)
-                for i in range(len(reqs)):
-                    cc(stream, dst[i], src[i])
-            else:
-                off = 0
-                for piece in binary_pieces(rows):
-                    view = src[off : off + piece]
-                    self.plans.get(key, piece)(stream, view, view, key[-1])
-                    off += piece
-            computed = torch.cuda.Event()
-            computed.record(stream)
-            self.download.wait_event(computed)
-            with torch.cuda.stream(self.download):
-                off = 0
-                for i, r in enumerate(reqs):
-                    if spec:
-                        part = dst[i]
-                    else:
-                        n = r.rows()
-                        part = dst[off : off + n] if key[0] == "fft1d" else dst[off]
-                        off += n
-                    r.result = r.out
-                    if r.result is None:
-                        r.result = torch.empty(tuple(part.shape), dtype=part.dtype, pin_memory=True)
-                    r.result.copy_(part, non_blocking=True)
+                    self._run_staged(key, reqs, plans, stream, g)
+        except Exception as e:  # noqa: BLE001
+            g.error = e
+            with torch.cuda.device(self.device):
+                # whatever was queued finishes before the buffers can go
+                for st in (self.upload, stream):
+                    ev = torch.cuda.Event()
+                    ev.record(st)
+                    self.download.wait_event(ev)
                 g.event = torch.cuda.Event()
                 g.event.record(self.download)
         for r in reqs:
-            r.launched = now
-        self._staged += need
+            r.event = g.event
+        self._staged += g.bytes
         self._inflight[s].append(g)
         self.groups += 1
+
+    def _run_direct(self, key, reqs, plans, stream, g) -> None:
+        """Device-resident requests with device outputs: no staging, each request is
+        transformed from its input straight into its output on the class's stream,
+        after the submitter's stream reached the point of submission."""
+        import torch
+
+        for r in reqs:
+            if r.ready is not None:
+                stream.wait_event(r.ready)
+            r.data.record_stream(stream)
+            r.out.record_stream(stream)
+            if key[0] == "spectrogram":
+                plans[1](stream, r.out, r.data)
+            elif key[0] == "fft2d":
+                plans[1](stream, r.out[None], r.data[None], key[-1])
+            else:
+                off = 0
+                for piece in binary_pieces(r.rows()):
+                    plans[piece](stream, r.out[off : off + piece], r.data[off : off + piece], key[-1])
+                    off += piece
+            r.result = r.out
+        g.event = torch.cuda.Event()
+        g.event.record(stream)
+
+    def _run_staged(self, key, reqs, plans, stream, g) -> None:
+        import torch
+
+        spec = key[0] == "spectrogram"
+        with torch.cuda.stream(self.upload):
+            for r in reqs:
+                if r.ready is not None:
+                    self.upload.wait_event(r.ready)
+                if getattr(r.data, "is_cuda", False):
+                    r.data.record_stream(self.upload)
+            if spec:
+                fr, bins = reqs[0].out_shape()
+                src = self._alloc((len(reqs), key[1]), torch.float32)
+                dst = self._alloc((len(reqs), fr, bins), torch.float32)
+                for i, r in enumerate(reqs):
+                    src[i].copy_(r.data, non_blocking=True)
+                g.buffers = [src, dst]
+            else:
+                rows = sum(r.rows() for r in reqs)
+                shape = (rows, key[1]) if key[0] == "fft1d" else (rows, key[1], key[2])
+                src = dst = self._alloc(shape, torch.complex64)
+                g.buffers = [src]
+                off = 0
+                for r in reqs:
+                    n = r.rows()
+                    (src[off : off + n] if key[0] == "fft1d" else src[off]).copy_(r.data, non_blocking=True)
+                    off += n
+            uploaded = torch.cuda.Event()
+            uploaded.record(self.upload)
+        stream.wait_event(uploaded)
+        if spec:
+            for i in range(len(reqs)):
+                plans[1](stream, dst[i], src[i])
+        else:
+            off = 0
+            for piece in binary_pieces(rows):
+                view = src[off : off + piece]
+                plans[piece](stream, view, view, key[-1])
+                off += piece
+        computed = torch.cuda.Event()
+        computed.record(stream)
+        self.download.wait_event(computed)
+        with torch.cuda.stream(self.download):
+            off = 0
+            for i, r in enumerate(reqs):
+                if spec:
+                    part = dst[i]
+                else:
+                    n = r.rows()
+                    part = dst[off : off + n] if key[0] == "fft1d" else dst[off]
+                    off += n
+                r.result = r.out
+                if r.result is None:
+                    r.result = torch.empty(tuple(part.shape), dtype=part.dtype, pin_memory=True)
+                elif getattr(r.result, "is_cuda", False):
+                    r.result.record_stream(self.download)
+                r.result.copy_(part, non_blocking=True)
+            g.event = torch.cuda.Event()
+            g.event.record(self.download)
 
     def _retire(self) -> None:
         now = None
         for d in self._inflight:
-            while d and d[0].event.query():
+            while d and (d[0].event is None or d[0].event.query()):
                 g = d.popleft()
                 now = time.perf_counter() if now is None else now
-                for r in g.requests:
-                    r.finished = now
-                    r.done = True
-                self.completed += len(g.requests)
+                if g.error is not None:
+                    self._fail(g.requests, g.error)
+                else:
+                    for r in g.requests:
+                        r.finished, r.done, r.status = now, True, "done"
+                    self.completed += len(g.requests)
                 self._staged -= g.bytes
                 g.buffers = []
 

@@ -170,7 +170,10 @@ KW_CASES = [(7, 16), (100, 256), (127, 256), (1000, 2048)]
 
 
 def main(argv: list[str]) -> int:
-    root = Path(argv[1]) if len(argv) > 1 else Path("/root/reference")
+    if len(argv) != 2:
+        print(f"usage: python {Path(argv[0]).name} <path of a fjarri/reikna checkout>", file=sys.stderr)
+        return 2
+    root = Path(argv[1])
     ns = load_reference(root)
     pow2 = [2**k for k in range(1, 25)]
     radix = {

@@ -47,14 +47,20 @@ def test_split_tc_matches_fp64(rows):
     assert err < fft_bound(numpy.complex64, 1024)
 
 
-def test_split_tc_sixty_db_and_inverse():
+@pytest.mark.parametrize("rows", [512, 16384])
+def test_split_tc_sixty_db_and_inverse(rows):
+    """The precision workload's 60 dB variant (components +-10^U(-3,0)), up to the
+    full 16384 x 1024 configuration, forward and inverse."""
     from reikna_b200 import _native as N
 
     rng = numpy.random.default_rng(8)
-    x = _sixty_db(rng, (512, 1024))
+    x = _sixty_db(rng, (rows, 1024))
     ref = numpy.fft.fft(x.astype(numpy.complex128), axis=1)
-    y, _ = _run(x, N.FLAG_SPLIT_TC)
-    assert rel_l2(y, ref) < fft_bound(numpy.complex64, 1024)
+    y, ntc = _run(x, N.FLAG_SPLIT_TC)
+    assert ntc == 1
+    err = rel_l2(y, ref)
+    print(f"60 dB rows={rows}: split-TC rel-L2 {err:.3e}")
+    assert err < fft_bound(numpy.complex64, 1024)
     # per-element check on the small components too: within the FP32 path's error
     y32, _ = _run(x, 0)
     assert numpy.abs(y - ref).max() < 8 * max(numpy.abs(y32 - ref).max(), 1e-6)
