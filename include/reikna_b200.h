@@ -57,6 +57,9 @@ extern "C" {
 #define RK_FMT_F64_PAIR 6 /* two float64 arrays: real part, imaginary part */
 #define RK_FMT_I32 7   /* int32 (FFTShift only) */
 #define RK_FMT_C64_HALF 8 /* reserved */
+#define RK_FMT_CONST 9  /* input only: no array; every element is the edge's additive term
+                           (broadcast_const / broadcast_param on the FFT input) */
+#define RK_FMT_IGNORE 10 /* output only: no array; the values are dropped (ignore) */
 
 /* output post-operations (applied after scale) */
 #define RK_POST_NONE 0
@@ -124,6 +127,12 @@ typedef struct rk_edge {
     int32_t window_axis;
     int64_t window_len;
     int32_t conj;                 /* 1: conjugate the element (after scale) */
+    int32_t add_slot;             /* runtime scalar added after the scale, -1 = none */
+    double add_re, add_im;        /* constant added after the scale (with add_slot's value):
+                                     element = scale * value + add (add_const / add_param,
+                                     and the value of an RK_FMT_CONST input) */
+    int32_t post_slot;            /* runtime scalar whose real part is the norm order
+                                     (norm_param), -1 = post_param */
 } rk_edge;
 
 typedef struct rk_fft_desc {

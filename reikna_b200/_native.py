@@ -28,6 +28,8 @@ FMT_F64 = 4
 FMT_F32_PAIR = 5
 FMT_F64_PAIR = 6
 FMT_I32 = 7
+FMT_CONST = 9
+FMT_IGNORE = 10
 
 POST_NONE = 0
 POST_NORM = 1
@@ -105,6 +107,10 @@ class Edge(ctypes.Structure):
         ("window_axis", ctypes.c_int32),
         ("window_len", ctypes.c_int64),
         ("conj", ctypes.c_int32),
+        ("add_slot", ctypes.c_int32),
+        ("add_re", ctypes.c_double),
+        ("add_im", ctypes.c_double),
+        ("post_slot", ctypes.c_int32),
     ]
 
 

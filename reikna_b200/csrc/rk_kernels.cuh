@@ -182,9 +182,11 @@ __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, 
     using V = cplx<T>;
     V v = cmk<V>(T(0), T(0));
     const int64_t a = la.c * s.cA + j * s.jB;
+    bool inb = false;  // an element of the user's array (not padding)
     if (la.ok && a < s.ax_len) {
         int64_t u = a + s.ax_shift;
         if (u >= s.ax_len) u -= s.ax_len;
+        inb = u < s.ax_bound;
         if (RP && (s.flags & SF_RPAIR) && u < s.ax_bound) {
             // a real signal read as sample pairs (x[2u], x[2u+1]); a window covers the
             // sample index 2u / 2u + 1
@@ -240,6 +242,10 @@ __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, 
     }
     const int32_t f = s.flags;
     if (f & SF_SCALE) v = cmul(v, cmk<V>((T)s.scale_re, (T)s.scale_im));
+    if ((f & SF_ADD) && inb) {
+        v.x += (T)s.add_re;
+        v.y += (T)s.add_im;
+    }
     if (f & SF_PRE_CONJ) v = cconj(v);
     // the tables hold ax_len entries; beyond that the element is the zero padding
     if (a < s.ax_len) {
@@ -276,6 +282,10 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
     if (f & SF_CHIRP) v = cmul(v, reinterpret_cast<const V*>(s.chirp)[a]);
     if (f & SF_POST_CONJ) v = cconj(v);
     if (f & SF_SCALE) v = cmul(v, cmk<V>((T)s.scale_re, (T)s.scale_im));
+    if (f & SF_ADD) {
+        v.x += (T)s.add_re;
+        v.y += (T)s.add_im;
+    }
     int64_t u = a + s.ax_shift;
     if (u >= s.ax_len) u -= s.ax_len;
     if (u >= s.ax_bound) return;

@@ -238,6 +238,12 @@ static int pos_max(int dbl) { return dbl ? 8192 : 16384; }
 static int fmt_is_complex(int f) { return f == RK_FMT_C64 || f == RK_FMT_C128; }
 static int fmt_is_pair(int f) { return f == RK_FMT_F32_PAIR || f == RK_FMT_F64_PAIR; }
 static int fmt_is_real(int f) { return f == RK_FMT_F32 || f == RK_FMT_F64; }
+// arrays a side of this format reads or writes (RK_FMT_CONST / RK_FMT_IGNORE: none)
+static int fmt_arrays(int f) { return fmt_is_pair(f) ? 2 : (f == RK_FMT_CONST || f == RK_FMT_IGNORE) ? 0 : 1; }
+// an additive term (or a constant input) that only the general element path applies
+static bool edge_has_add(const rk_edge& e) {
+    return e.format == RK_FMT_CONST || e.add_slot >= 0 || e.add_re != 0.0 || e.add_im != 0.0;
+}
 
 // symbolic buffers while planning
 enum SymBuf { SB_IN = 0, SB_OUT = 1, SB_T0 = 2, SB_T1 = 3, SB_M0 = 4, SB_M1 = 5 };
@@ -301,6 +307,7 @@ static int half_eligible(const rk_fft_desc& d, int dbl) {
     const rk_edge& in = d.input;
     const rk_edge& out = d.output;
     const int rfmt = dbl ? RK_FMT_F64 : RK_FMT_F32, cfmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
+    if (edge_has_add(in) || edge_has_add(out)) return 0;
     if (in.format != rfmt || in.shape[ax] != n || in.shift[ax] != 0) return 0;
     if (in.window != RK_WIN_NONE && in.window_axis != ax) return 0;
     if (out.shift[ax] != 0 || out.shape[ax] > L + 1) return 0;
@@ -328,6 +335,10 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
     }
     if (real_flags && (d.naxes != 1 || d.axes[0] != nd - 1 || d.shape[nd - 1] < 8)) {
         set_error("a one-pass real transform needs a transform of the last axis only, of at least 8 points");
+        return RK_ERR_UNSUPPORTED;
+    }
+    if (real_flags && (edge_has_add(d.input) || edge_has_add(d.output) || d.output.format == RK_FMT_IGNORE)) {
+        set_error("a one-pass real transform takes no additive term, constant input or ignored output");
         return RK_ERR_UNSUPPORTED;
     }
     int cur = SB_IN;
@@ -681,6 +692,7 @@ static void build_side(const rk_fft_desc& d, const SideSpec& ss, int ax, int dbl
     s.scale_re = 1.0;
     s.scale_im = 0.0;
     if (e) {
+        if (edge_has_add(*e)) s.flags |= SF_ADD;  // value set per call
         if (is_load && e->window != RK_WIN_NONE && e->window_axis == ax) {
             s.flags |= SF_WINDOW;
             s.win_len = (int32_t)e->window_len;
@@ -695,7 +707,7 @@ static void build_side(const rk_fft_desc& d, const SideSpec& ss, int ax, int dbl
 // Mark a side for the lean block load/store path (load_block / store_block).
 static void mark_fast(Side& s, int dbl, int L) {
     const int fmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
-    const int32_t bad = SF_CHIRP | SF_TAB | SF_WINDOW | SF_NORM | SF_TW4;
+    const int32_t bad = SF_CHIRP | SF_TAB | SF_WINDOW | SF_NORM | SF_TW4 | SF_ADD;
     if (s.fmt == fmt && s.cA == 0 && s.jB == 1 && s.ax_len == L && s.ax_bound == s.ax_len && is_pow2(L) &&
         !(s.flags & bad) && s.ax_stride >= 0 && s.ax_stride * (int64_t)L < (int64_t(1) << 31))
         s.flags |= SF_FAST;
@@ -725,8 +737,9 @@ static void setup_tma(PassRec& r, int dbl, int nsm) {
         if (p.I % NL != 0 || ld.nd_i != 1 || ld.i_stride[0] != 1 || ld.i_shape[0] != p.I || ld.i_shift[0] != 0 ||
             ld.i_bound[0] != p.I || ld.nd_o > 1)
             return;
-        if ((ld.ax_stride * esz) % 16 != 0) return;
-        if (ld.nd_o == 1 && (ld.o_stride[0] * esz) % 16 != 0) return;
+        // (a broadcast input has zero strides: plain loads read it)
+        if (ld.ax_stride <= 0 || (ld.ax_stride * esz) % 16 != 0) return;
+        if (ld.nd_o == 1 && (ld.o_stride[0] <= 0 || (ld.o_stride[0] * esz) % 16 != 0)) return;
         if (ld.offset != 0) return;
         p.tma_mode = TMA_TENSOR;
         p.tma_boxes = (int)std::max<int64_t>(1, L / 256);
@@ -754,7 +767,7 @@ static void setup_tma(PassRec& r, int dbl, int nsm) {
 static void mark_fast2(Side& s, int dbl, int64_t L, int64_t C) {
     if (s.flags & SF_FAST) return;
     const int fmt = dbl ? RK_FMT_C128 : RK_FMT_C64;
-    if (s.fmt != fmt || s.ax_shift != 0 || (s.flags & (SF_WINDOW | SF_NORM))) return;
+    if (s.fmt != fmt || s.ax_shift != 0 || (s.flags & (SF_WINDOW | SF_NORM | SF_ADD))) return;
     if (s.cA < 0 || s.jB < 0 || s.ax_stride < 0) return;
     const int64_t amax = (C - 1) * s.cA + (L - 1) * s.jB;
     const int64_t lim = int64_t(1) << 31;
@@ -808,10 +821,20 @@ static int validate(const rk_fft_desc* d) {
                 return RK_ERR_INVALID;
             }
         }
-        if (!(fmt_is_complex(e->format) || fmt_is_real(e->format) || fmt_is_pair(e->format))) {
+        const bool special = (e == &d->input && e->format == RK_FMT_CONST) ||
+                             (e == &d->output && e->format == RK_FMT_IGNORE);
+        if (!(fmt_is_complex(e->format) || fmt_is_real(e->format) || fmt_is_pair(e->format) || special)) {
             set_error("unsupported edge format");
             return RK_ERR_INVALID;
         }
+        if (e->add_slot < -1 || e->post_slot < -1 || e->scale_slot < -1 || e->scale_div_slot < -1) {
+            set_error("scalar slots are -1 (none) or a slot index");
+            return RK_ERR_INVALID;
+        }
+    }
+    if (d->input.post_slot >= 0) {
+        set_error("a norm order slot belongs to the output edge");
+        return RK_ERR_INVALID;
     }
     if (fmt_is_real(d->output.format) && d->output.post != RK_POST_NORM) {
         set_error("real output requires a norm post-operation");
@@ -861,6 +884,7 @@ static std::string describe_json(const rk_fft_desc& d, const Planned& P) {
 }
 
 static int64_t edge_extent_bytes(const rk_edge& e, int second) {
+    if (!fmt_arrays(e.format)) return 0;
     int esz = 8;
     switch (e.format) {
         case RK_FMT_C64: esz = 8; break;
@@ -986,6 +1010,10 @@ int rk_edge_init(rk_edge* e, int32_t format, int32_t ndim, const int64_t* shape)
     e->post = RK_POST_NONE;
     e->post_param = 2.0;
     e->window = RK_WIN_NONE;
+    e->add_slot = -1;
+    e->add_re = 0.0;
+    e->add_im = 0.0;
+    e->post_slot = -1;
     return RK_OK;
 }
 
@@ -1410,9 +1438,9 @@ int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs
                       std::vector<PassParams>& out, std::vector<char>* tma_ok) {
     if (!plan) { set_error("null plan"); return RK_ERR_INVALID; }
     const rk_fft_desc& d = plan->desc;
-    const int need_in = fmt_is_pair(d.input.format) ? 2 : 1;
-    const int need_out = fmt_is_pair(d.output.format) ? 2 : 1;
-    if (!inputs || !outputs || n_inputs < need_in || n_outputs < need_out) {
+    const int need_in = fmt_arrays(d.input.format);
+    const int need_out = fmt_arrays(d.output.format);
+    if ((need_in && !inputs) || (need_out && !outputs) || n_inputs < need_in || n_outputs < need_out) {
         set_error("wrong number of input/output arrays");
         return RK_ERR_INVALID;
     }
@@ -1420,12 +1448,14 @@ int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs
         if (!inputs[i]) { set_error("null input pointer"); return RK_ERR_INVALID; }
     for (int i = 0; i < need_out; ++i)
         if (!outputs[i]) { set_error("null output pointer"); return RK_ERR_INVALID; }
-    const void* in0 = inputs[0];
+    const void* in0 = need_in ? inputs[0] : nullptr;
     const void* in1 = need_in > 1 ? inputs[1] : nullptr;
+    void* out0 = need_out ? outputs[0] : nullptr;
+    void* out1 = need_out > 1 ? outputs[1] : nullptr;
 
     // in-place call of a single remapping pass: read from a private copy
-    if (plan->alias_hazard && (in0 == outputs[0] || (in1 && (in1 == outputs[0] || (need_out > 1 && in1 == outputs[1]))) ||
-                               (need_out > 1 && in0 == outputs[1]))) {
+    if (plan->alias_hazard && in0 && out0 &&
+        (in0 == out0 || (in1 && (in1 == out0 || (out1 && in1 == out1))) || (out1 && in0 == out1))) {
         const int64_t need = plan->in_extent_bytes + plan->in2_extent_bytes + 256;
         if (!plan->alias_tmp) {
             cudaError_t e = cudaMalloc(&plan->alias_tmp, (size_t)need);
@@ -1449,6 +1479,22 @@ int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs
     double in_re, in_im, out_re, out_im;
     apply_edge_scale(d.input, scalars, n_scalars, in_re, in_im, &bad);
     apply_edge_scale(d.output, scalars, n_scalars, out_re, out_im, &bad);
+    // additive terms: the constant plus the slot's value; applied after the scale,
+    // so the inverse's 1/N (a factor of the output scale) does not touch them
+    double add_in[2] = {d.input.add_re, d.input.add_im}, add_out[2] = {d.output.add_re, d.output.add_im};
+    for (int k = 0; k < 2; ++k) {
+        const rk_edge& e = k ? d.output : d.input;
+        double* a = k ? add_out : add_in;
+        if (e.add_slot >= 0) {
+            if (e.add_slot >= n_scalars) { bad = 1; continue; }
+            a[0] += scalars[2 * e.add_slot];
+            a[1] += scalars[2 * e.add_slot + 1];
+        }
+    }
+    double order = d.output.post_param;
+    if (d.output.post_slot >= 0) {
+        if (d.output.post_slot >= n_scalars) bad = 1; else order = scalars[2 * d.output.post_slot];
+    }
     if (bad) { set_error("scalar slot out of range"); return RK_ERR_INVALID; }
     if (inverse) {
         out_re /= plan->n_total;
@@ -1482,16 +1528,21 @@ int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs
                 p.ld.scale_re = in_re;
                 p.ld.scale_im = in_im;
             }
+            p.ld.add_re = add_in[0];
+            p.ld.add_im = add_in[1];
             if (d.input.conj) p.ld.flags ^= SF_PRE_CONJ;
         }
         if (r.st_edge) {
-            p.st.ptr = outputs[0];
-            p.st.ptr2 = need_out > 1 ? outputs[1] : nullptr;
+            p.st.ptr = out0;
+            p.st.ptr2 = out1;
             if (out_re != 1.0 || out_im != 0.0) {
                 p.st.flags |= SF_SCALE;
                 p.st.scale_re = out_re;
                 p.st.scale_im = out_im;
             }
+            p.st.add_re = add_out[0];
+            p.st.add_im = add_out[1];
+            if (p.st.flags & SF_NORM) p.st.post_param = order;
         }
         if (inverse) {
             // IFFT(x) = conj(FFT(conj(x))) / N: conjugate on the first load and last store

@@ -26,6 +26,7 @@ enum SideFlags : int32_t {
     SF_FAST2 = 512,     // pass-dtype side, a = c cA + j jB, no remap, 32-bit offsets
     SF_FASTR = 1024,    // real side of the pass precision, a = j, no remap, 32-bit offsets
     SF_RPAIR = 2048,    // real load side read as sample pairs: element u = x[2u] + i x[2u+1]
+    SF_ADD = 4096,      // add (add_re + i add_im) after the scale (user elements only)
 };
 
 // Addressing of one buffer in a pass.  A line l in [0, O*C*I) decomposes as
@@ -48,6 +49,7 @@ struct Side {
     int32_t ax_shift;
     int32_t win_len;
     double scale_re, scale_im;
+    double add_re, add_im;
     double post_param;
     const void* chirp;
     const void* tab;

@@ -14,7 +14,7 @@ import numpy
 from .. import _native as N
 from ..core.computation import Computation, array_pointer, scalar_value
 from ..core.signature import Annotation, ArrayMetadata, Parameter, Type
-from ._fold import edge_struct, fold_input, fold_output
+from ._fold import fold_input, fold_output, native_edges
 
 
 def _is_complex(dtype) -> bool:
@@ -53,11 +53,11 @@ class FFT(Computation):
         meta = self._meta
         tree = self._tr_tree
         shape = tuple(meta.shape)
-        ispec = fold_input(tree, "input", shape)
-        ospec = fold_output(tree, "output", shape)
+        ispec = fold_input(tree, "input", shape, meta.dtype)
+        ospec = fold_output(tree, "output", shape, meta.dtype)
         leaves = tree.get_leaf_parameters()
         scalar_names = [p.name for p in leaves if p.annotation.is_scalar() and p.name != "inverse"]
-        slots = {name: i for i, name in enumerate(scalar_names)}
+        ein, eout, scalars = native_edges(ispec, ospec, scalar_names)
         d = N.FftDesc()
         d.dtype = N.FMT_C64 if meta.dtype == numpy.complex64 else N.FMT_C128
         d.ndim = len(shape)
@@ -67,9 +67,9 @@ class FFT(Computation):
         for i, a in enumerate(self._axes):
             d.axes[i] = a
         d.flags = flags
-        d.input = edge_struct(ispec, slots)
-        d.output = edge_struct(ospec, slots)
-        return d, ispec, ospec, scalar_names
+        d.input = ein
+        d.output = eout
+        return d, ispec, ospec, scalar_names, scalars
 
     def describe(self, flags: int = 0) -> dict:
         """Kernel chain the native planner builds for this computation (no GPU needed)."""
@@ -77,7 +77,7 @@ class FFT(Computation):
         return N.describe(d)
 
     def _build_runner(self, device, flags: int = 0, **_ignored):
-        d, ispec, ospec, scalar_names = self.native_descriptor(flags)
+        d, ispec, ospec, scalar_names, scalar_list = self.native_descriptor(flags)
         plan = N.Plan(d)
         ann = {p.name: p.annotation for p in self._tr_tree.get_leaf_parameters()}
 
@@ -85,7 +85,7 @@ class FFT(Computation):
             """(output pointers, input pointers, inverse, scalars) of one call."""
             outs = [array_pointer(args[n], ann[n]) for n in ospec.arrays]
             ins = [array_pointer(args[n], ann[n]) for n in ispec.arrays]
-            scalars = [scalar_value(args[n]) for n in scalar_names]
+            scalars = scalar_list({n: scalar_value(args[n]) for n in scalar_names})
             return outs, ins, int(args["inverse"]), scalars
 
         def runner(stream: int, args):

@@ -64,14 +64,14 @@ class FFTShift(Computation):
             return runner
 
         # general route: a native plan with no transformed axes and an output remap
-        from ..fft._fold import edge_struct, fold_input, fold_output
+        from ..fft._fold import fold_input, fold_output, native_edges
 
         if not numpy.dtype(meta.dtype).kind == "c":
             raise NotImplementedError("FFTShift with transformations supports complex arrays only")
-        ispec = fold_input(tree, "input", shape)
-        ospec = fold_output(tree, "output", shape)
+        ispec = fold_input(tree, "input", shape, meta.dtype)
+        ospec = fold_output(tree, "output", shape, meta.dtype)
         scalar_names = [p.name for p in leaves if p.annotation.is_scalar() and p.name != "inverse"]
-        slots = {n: i for i, n in enumerate(scalar_names)}
+        ein, eout, scalar_list = native_edges(ispec, ospec, scalar_names)
         plans = {}
         ann = {p.name: p.annotation for p in leaves}
 
@@ -82,8 +82,8 @@ class FFTShift(Computation):
             for i, s in enumerate(shape):
                 d.shape[i] = s
             d.naxes = 0
-            d.input = edge_struct(ispec, slots)
-            o = edge_struct(ospec, slots)
+            d.input = ein
+            o = N.Edge.from_buffer_copy(eout)
             for a in self._axes:
                 n = shape[a]
                 s = (n + 1) // 2 if inverse else n // 2
@@ -97,7 +97,7 @@ class FFTShift(Computation):
                 plans[inv] = make(inv)
             outs = [array_pointer(args[n], ann[n]) for n in ospec.arrays]
             ins = [array_pointer(args[n], ann[n]) for n in ispec.arrays]
-            scalars = [complex(numpy.asarray(args[n]).item()) for n in scalar_names]
+            scalars = scalar_list({n: complex(numpy.asarray(args[n]).item()) for n in scalar_names})
             plans[inv].execute(outs, ins, inverse=0, scalars=scalars, stream=stream)
 
         runner.launches = 1

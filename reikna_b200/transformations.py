@@ -6,7 +6,8 @@ define for the FFT hot path: ``fftshift`` (examples/demo_fftshift_transformation
 ``real_to_complex`` (examples/demo_real_to_complex_fft.py:20), and the spectrogram
 pieces ``rolling_frame``, ``hanning_window`` and ``crop_frequencies``
 (examples/demo_specgram.py:97-193).  Each carries an ``op`` descriptor that the FFT
-planner fuses into its first load or last store.
+planner fuses into its first load or last store; every one of them can be connected
+to an FFT's input or output (the ones that make sense on that side).
 """
 
 from __future__ import annotations
@@ -90,7 +91,7 @@ def div_const(arr_t, param) -> Transformation:
 
 
 def add_param(arr_t, param_dtype) -> Transformation:
-    """Addition of a runtime scalar (not fusable into FFT passes)."""
+    """Addition of a runtime scalar (1 output, 1 input, 1 scalar): ``output = input + param``."""
     inp = _meta(arr_t)
     return Transformation(
         [
@@ -103,7 +104,7 @@ def add_param(arr_t, param_dtype) -> Transformation:
 
 
 def add_const(arr_t, param) -> Transformation:
-    """Addition of a constant (not fusable into FFT passes)."""
+    """Addition of a constant (1 output, 1 input): ``output = input + param``."""
     inp = _meta(arr_t)
     return Transformation(
         [Parameter("output", Annotation(inp, "o")), Parameter("input", Annotation(inp, "i"))],
@@ -153,7 +154,7 @@ def norm_const(arr_t, order) -> Transformation:
 
 
 def norm_param(arr_t) -> Transformation:
-    """``output = abs(input) ** order`` with a runtime order (not fusable)."""
+    """``output = abs(input) ** order`` with a runtime ``order`` (1 output, 1 input, 1 scalar)."""
     inp = _meta(arr_t)
     out_dtype = real_for(inp.dtype)
     return Transformation(
@@ -181,7 +182,7 @@ def broadcast_const(arr_t, val) -> Transformation:
 
 
 def broadcast_param(arr_t) -> Transformation:
-    """Broadcasts a runtime scalar to the array output (not fusable)."""
+    """Broadcasts a runtime scalar ``param`` to the array output (1 output, 1 scalar)."""
     inp = _meta(arr_t)
     return Transformation(
         [Parameter("output", Annotation(inp, "o")), Parameter("param", Annotation(inp.dtype))],

@@ -50,7 +50,7 @@ def test_connect_returns_computation_and_is_chainable():
     assert res is fft
     fft.parameter.out1.connect(t2, t2.input, out2=t2.output, scale=t2.param)
     assert names(fft) == ["out2", "scale", "input", "inverse"]
-    d, ispec, ospec, scalars = fft.native_descriptor()
+    d, ispec, ospec, scalars, _ = fft.native_descriptor()
     assert scalars == ["scale"]
     assert d.output.scale_re == 2.0 and d.output.scale_div_slot == 0
 
@@ -114,7 +114,7 @@ def test_split_and_combine_fold():
     fft.parameter.input.connect(cc, cc.output, in_re=cc.real, in_im=cc.imag)
     fft.parameter.output.connect(sc, sc.input, out_re=sc.real, out_im=sc.imag)
     assert names(fft) == ["out_re", "out_im", "in_re", "in_im", "inverse"]
-    d, ispec, ospec, _ = fft.native_descriptor()
+    d, ispec, ospec, *_ = fft.native_descriptor()
     assert d.input.format == N.FMT_F32_PAIR and d.output.format == N.FMT_F32_PAIR
     assert ispec.arrays == ["in_re", "in_im"] and ospec.arrays == ["out_re", "out_im"]
 
@@ -138,7 +138,7 @@ def test_spectrogram_chain_fold():
     fft.parameter.output.connect(amp, amp.parameter.input, amplitude=amp.parameter.output)
     fft.parameter.amplitude.connect(crop, crop.parameter.input, cropped_amplitude=crop.parameter.output)
     assert names(fft) == ["cropped_amplitude", "flat_input", "inverse"]
-    d, ispec, ospec, _ = fft.native_descriptor()
+    d, ispec, ospec, *_ = fft.native_descriptor()
     assert d.input.format == N.FMT_F32
     assert list(d.input.strides)[:2] == [256, 1]
     assert list(d.input.shape)[:2] == [13, 1024]
@@ -185,3 +185,63 @@ def test_torch_tensor_metadata():
 def test_fftshift_signature():
     s = FFTShift(meta((10, 11)), axes=(0, 1))
     assert names(s) == ["output", "input", "inverse"]
+
+
+# ---- the whole built-in set folds into the edges ----------------------------------
+
+
+def test_affine_chain_folds_constants():
+    arr = meta((32,))
+    fft = FFT(arr)
+    a = tr.add_const(arr, 1 + 2j)
+    m = tr.mul_const(arr, 3.0)
+    # output -> add (1+2i) -> mul 3 -> leaf: leaf = 3 y + 3 (1 + 2i)
+    fft.parameter.output.connect(a, a.input, o1=a.output)
+    fft.parameter.o1.connect(m, m.input, o2=m.output)
+    d, ispec, ospec, names_, scal = fft.native_descriptor()
+    assert (d.output.scale_re, d.output.scale_im) == (3.0, 0.0)
+    assert (d.output.add_re, d.output.add_im) == (3.0, 6.0) and d.output.add_slot == -1
+    assert scal({}) == []
+
+
+def test_affine_chain_with_runtime_scalars_uses_extra_slots():
+    arr = meta((32,))
+    fft = FFT(arr)
+    mp = tr.mul_param(arr, numpy.complex64)
+    ap = tr.add_param(arr, numpy.float32)
+    # input chain: fft_in = p * (x + q)
+    fft.parameter.input.connect(mp, mp.output, x1=mp.input, p=mp.param)
+    fft.parameter.x1.connect(ap, ap.output, x=ap.input, q=ap.param)
+    d, ispec, ospec, names_, scal = fft.native_descriptor()
+    assert sorted(names_) == ["p", "q"]
+    assert d.input.scale_slot == names_.index("p") and d.input.add_slot == 2
+    vals = scal({"p": 2j, "q": 0.5})
+    assert vals[names_.index("p")] == 2j and vals[2] == 1j
+
+
+def test_constant_sources_and_sinks():
+    arr = meta((16, 8))
+    fft = FFT(arr)
+    bc = tr.broadcast_param(arr)
+    fft.parameter.input.connect(bc, bc.output, value=bc.param)
+    ig = tr.ignore(arr)
+    fft.parameter.output.connect(ig, ig.input)
+    assert names(fft) == ["value", "inverse"]
+    d, ispec, ospec, names_, scal = fft.native_descriptor()
+    assert d.input.format == N.FMT_CONST and d.input.add_slot == 1 and ispec.arrays == []
+    assert d.output.format == N.FMT_IGNORE and ospec.arrays == []
+    assert scal({"value": 2 + 1j}) == [2 + 1j, 2 + 1j]
+    assert fft.describe()["passes"]
+
+
+def test_norm_param_and_copy_broadcasted():
+    arr = meta((8, 16))
+    fft = FFT(arr)
+    npm = tr.norm_param(arr)
+    fft.parameter.output.connect(npm, npm.input, mag=npm.output, order=npm.order)
+    row = ArrayMetadata((16,), numpy.complex64)
+    cb = tr.copy_broadcasted(row, arr)
+    fft.parameter.input.connect(cb, cb.output, row=cb.input)
+    d, ispec, *_ = fft.native_descriptor()
+    assert d.output.post == N.POST_NORM and d.output.post_slot == 0
+    assert list(d.input.strides)[:2] == [0, 1] and list(d.input.shape)[:2] == [8, 16]
