@@ -26,7 +26,9 @@
 #ifndef REIKNA_B200_H
 #define REIKNA_B200_H
 
+#ifndef __CUDACC_RTC__
 #include <stdint.h>
+#endif
 
 #if defined(__GNUC__)
 #define RK_API __attribute__((visibility("default")))
@@ -60,6 +62,12 @@ extern "C" {
 #define RK_FMT_CONST 9  /* input only: no array; every element is the edge's additive term
                            (broadcast_const / broadcast_param on the FFT input) */
 #define RK_FMT_IGNORE 10 /* output only: no array; the values are dropped (ignore) */
+#define RK_FMT_USER 11  /* the element is produced (input) or consumed (output) by device
+                           code compiled at run time for this plan (a transformation given as
+                           source code): strides must be the C-order strides of the FFT shape
+                           (the code receives the flat index), offset 0, no remap; passes that
+                           touch such an edge run only with a kernel installed by
+                           rk_fft_plan_set_pass_kernel */
 
 /* output post-operations (applied after scale) */
 #define RK_POST_NONE 0
@@ -166,6 +174,33 @@ RK_API int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_out
                    const double* scalars, int32_t n_scalars, void* stream);
 
 RK_API int rk_fft_plan_destroy(rk_fft_plan* plan);
+
+/*
+ * Transformations given as source code (reikna's Transformation(parameters, code),
+ * reikna/core/transformation.py:42-120, inlined by reikna into the first and last
+ * kernel, reikna/core/transformation_modules.py:260-318).  An edge of format
+ * RK_FMT_USER is read or written by device functions compiled at run time together
+ * with the pass kernel that calls them; the host compiles one kernel per pass that
+ * touches such an edge and installs it here.
+ *
+ * rk_fft_plan_pass_info: info[0..7] = {kind (0 line, 1 plane), L, mode (0 position,
+ *   1 lane), variant, complex128 (0/1), threads per CTA, user bits (1: the pass loads
+ *   the input edge's user code, 2: it stores through the output edge's), lines per
+ *   CTA}; *smem = dynamic shared memory bytes of a CTA.
+ * rk_fft_plan_set_pass_kernel: load a cubin `image` (size bytes) holding the
+ *   extern "C" kernel `name` with the pass's launch shape and a single
+ *   `rk::PassParams` argument, and run pass `index` with it from now on.
+ * rk_fft_execute_user: rk_fft_execute plus up to 8 64-bit words per edge handed to
+ *   the user code (array pointers and scalar bit patterns, as the host that generated
+ *   the code laid them out).
+ */
+RK_API int rk_fft_plan_pass_info(const rk_fft_plan* plan, int32_t index, int32_t* info, int64_t* smem);
+RK_API int rk_fft_plan_set_pass_kernel(rk_fft_plan* plan, int32_t index, const void* image, int64_t size,
+                                       const char* name);
+RK_API int rk_fft_execute_user(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
+                               int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars,
+                               const uint64_t* user_in, int32_t n_user_in, const uint64_t* user_out,
+                               int32_t n_user_out, void* stream);
 
 /* Device bytes owned by the plan (temporaries + tables). */
 RK_API int rk_fft_plan_device_bytes(const rk_fft_plan* plan, int64_t* bytes);

@@ -18,7 +18,7 @@ from typing import Any
 
 import numpy
 
-from .signature import Parameter, Signature, Type, as_numpy_dtype
+from .signature import Annotation, Parameter, Signature, Type, as_numpy_dtype
 from .transformation import Transformation, TransformationParameter, TransformationTree
 
 
@@ -93,8 +93,14 @@ class Computation:
         self._update_attributes()
         return self
 
-    def compile(self, device=None, **kwds) -> ComputationCallable:
-        """Plan and build the native kernels on ``device`` (torch device, index or None)."""
+    def compile(self, device=None, compiler_options=(), *, fast_math: bool = False, keep: bool = False,
+                **kwds) -> ComputationCallable:
+        """Plan and build the native kernels on ``device`` (torch device, index or None).
+
+        ``compiler_options``, ``fast_math`` and ``keep`` are reikna's compile options
+        (reikna/core/computation.py:259-287); they apply to the kernels this library
+        compiles at run time (user transformations), the prebuilt ones ignore them.
+        Other keywords (``flags``) go to the native planner."""
         import torch
 
         if device is None:
@@ -105,12 +111,36 @@ class Computation:
             device = torch.device(device)
         if device.type != "cuda":
             raise ValueError("reikna_b200 computations run on CUDA devices only")
+        self._compile_options = {"compiler_options": list(compiler_options), "fast_math": bool(fast_math),
+                                 "keep": bool(keep)}
         with torch.cuda.device(device):
+            if type(self)._build_plan is not Computation._build_plan:
+                return self._compile_plan(device, **kwds)
             runner = self._build_runner(device, **kwds)
         return ComputationCallable(device, self._tr_tree.get_leaf_parameters(), runner)
 
     def _build_runner(self, device, **kwds) -> Callable:
         raise NotImplementedError
+
+    # -- computations composed of other computations (reikna's ComputationPlan) ------
+    def _build_plan(self, plan_factory, device_params, args) -> ComputationPlan:
+        """Derived classes that compose other computations override this (see
+        reikna/core/computation.py:289-308): record temporaries and nested computation
+        calls on ``plan_factory()`` and return the plan."""
+        raise NotImplementedError
+
+    def _compile_plan(self, device, **kwds) -> ComputationCallable:
+        for name, node in self._tr_tree.nodes.items():
+            if node.input_ntr is not None or node.output_ntr is not None:
+                if name in {p.name for p in self._original_parameters}:
+                    raise NotImplementedError(
+                        "transformations connected to a computation built from nested calls; connect them to "
+                        "the nested computations instead")
+        args = KernelArguments({p.name: KernelArgument(p.name, p.annotation) for p in self._original_parameters})
+        plan = self._build_plan(lambda: ComputationPlan(self, device, kwds), DeviceParameters(device), args)
+        if not isinstance(plan, ComputationPlan):
+            raise TypeError("_build_plan() must return the plan it was given")
+        return plan.finalize()
 
 
 def stream_handle(stream) -> int:
@@ -166,3 +196,165 @@ class ComputationCallable:
 
 def scalar_value(v) -> complex:
     return complex(numpy.asarray(v).item())
+
+
+# ---- nested computations ---------------------------------------------------------------
+
+
+class DeviceParameters:
+    """What ``_build_plan`` learns about the device (grunnur's DeviceParameters
+    subset that host-side planning uses)."""
+
+    def __init__(self, device):
+        import torch
+
+        pr = torch.cuda.get_device_properties(device)
+        self.device = device
+        self.api_id = "cuda"
+        self.warp_size = 32
+        self.max_total_local_size = 1024
+        self.local_mem_size = 227 * 1024
+        self.compute_units = pr.multi_processor_count
+        self.type = "gpu"
+
+
+class KernelArgument(Type):
+    """A value a plan passes to a nested call: a root parameter of the computation,
+    a temporary, a persistent array or a persistent scalar."""
+
+    def __init__(self, name: str, type_):
+        super().__init__(type_)
+        self.name = name
+
+    def __repr__(self):
+        return f"KernelArgument({self.name})"
+
+
+class KernelArguments:
+    def __init__(self, args):
+        self._args = dict(args)
+
+    def all(self):
+        return self._args.values()
+
+    def __getattr__(self, name: str) -> KernelArgument:
+        try:
+            return self._args[name]
+        except KeyError as exc:
+            raise AttributeError(name) from exc
+
+
+class ComputationPlan:
+    """Recorder of a composed computation (reikna/core/computation.py:346-640):
+    temporaries, persistent and constant arrays, and nested computation calls, run
+    in order on the caller's stream.  Each nested computation is compiled for the
+    device when it is recorded; a temporary is allocated once when the plan is
+    finalized and lives as long as the compiled callable."""
+
+    def __init__(self, owner: Computation, device, kwds):
+        self._owner = owner
+        self._device = device
+        self._kwds = dict(kwds)
+        self._annotations = {p.name: p.annotation for p in owner._original_parameters}
+        self._temps: dict[str, Annotation] = {}
+        self._values: dict[str, Any] = {}
+        self._calls: list[tuple[ComputationCallable, list[str]]] = []
+        self._ids = {"temp": 0, "value": 0}
+
+    def _new(self, kind: str) -> str:
+        self._ids[kind] += 1
+        return f"_{kind}{self._ids[kind]}"
+
+    def temp_array(self, shape, dtype, strides=None, offset: int = 0, nbytes=None) -> KernelArgument:
+        from .signature import ArrayMetadata
+
+        shape = (shape,) if isinstance(shape, int) else tuple(shape)
+        meta = ArrayMetadata(shape, dtype, strides=strides, first_element_offset=offset, buffer_size=nbytes)
+        name = self._new("temp")
+        ann = Annotation(meta, "io")
+        self._annotations[name] = ann
+        self._temps[name] = ann
+        return KernelArgument(name, ann)
+
+    def temp_array_like(self, arr) -> KernelArgument:
+        from .signature import ArrayMetadata
+
+        meta = arr.as_array_metadata() if hasattr(arr, "as_array_metadata") else ArrayMetadata.from_arraylike(arr)
+        return self.temp_array(meta.shape, meta.dtype, strides=meta.strides, offset=meta.first_element_offset,
+                               nbytes=meta.buffer_size)
+
+    def persistent_array(self, arr) -> KernelArgument:
+        import torch
+
+        from .signature import ArrayMetadata
+
+        t = torch.as_tensor(numpy.ascontiguousarray(arr)).to(self._device)
+        name = self._new("value")
+        ann = Annotation(ArrayMetadata.from_arraylike(t), "i")
+        self._annotations[name] = ann
+        self._values[name] = t
+        return KernelArgument(name, ann)
+
+    constant_array = persistent_array
+
+    def _scalar(self, annotation, value) -> KernelArgument:
+        name = self._new("value")
+        ann = Annotation(annotation.dtype)
+        self._annotations[name] = ann
+        self._values[name] = annotation.cast_scalar(value)
+        return KernelArgument(name, ann)
+
+    def computation_call(self, computation: Computation, *args, **kwds) -> None:
+        """Add a call of ``computation`` with ``args``: plan arguments, or scalars
+        (kept as persistent values)."""
+        sig = computation.signature
+        bound = sig.bind_with_defaults(args, kwds, cast=False)
+        names = []
+        for arg, param in zip(bound.args, sig.parameters.values()):
+            if not isinstance(arg, KernelArgument):
+                if param.annotation.is_array():
+                    raise ValueError("Ad hoc arguments are only allowed for scalar parameters")
+                arg = self._scalar(param.annotation, arg)
+            ann = self._annotations.get(arg.name)
+            if ann is None:
+                raise ValueError(f"'{arg.name}' is not an argument of this plan")
+            if not ann.can_be_argument_for(param.annotation):
+                raise ValueError(f"Got {ann} for '{param.name}', expected {param.annotation}")
+            names.append(arg.name)
+        opts = getattr(self._owner, "_compile_options", {})
+        cc = computation.compile(self._device, opts.get("compiler_options", ()), fast_math=opts.get("fast_math", False),
+                                 keep=opts.get("keep", False), **self._kwds)
+        self._calls.append((cc, names))
+
+    def kernel_call(self, template_def, args, global_size, local_size=None, render_kwds=None,
+                    kernel_name="_kernel_func"):
+        raise NotImplementedError(
+            "kernel_call: this library runs prebuilt sm_100a kernels; compose computations with computation_call")
+
+    def finalize(self) -> ComputationCallable:
+        import torch
+
+        internal = dict(self._values)
+        for name, ann in self._temps.items():
+            meta = ann.as_array_metadata()
+            isz = meta.dtype.itemsize
+            span = meta.first_element_offset + sum((n - 1) * st for n, st in zip(meta.shape, meta.strides)) + isz
+            nbytes = max(meta.buffer_size or 0, span)
+            buf = torch.empty(nbytes, dtype=torch.uint8, device=self._device)
+            from .signature import _torch_dtype_map
+
+            tdt = _torch_dtype_map()[numpy.dtype(meta.dtype)]
+            internal[name] = torch.as_strided(buf.view(tdt), meta.shape, [st // isz for st in meta.strides],
+                                              meta.first_element_offset // isz)
+        calls = self._calls
+
+        def runner(stream: int, args):
+            vals = dict(internal)
+            vals.update(args)
+            ext = torch.cuda.ExternalStream(stream) if stream else None
+            for cc, names in calls:
+                cc(ext, *[vals[n] for n in names])
+
+        runner.launches = sum(cc.launches for cc, _ in calls)
+        runner.internal = internal
+        return ComputationCallable(self._device, self._owner._tr_tree.get_leaf_parameters(), runner)

@@ -182,7 +182,8 @@ __global__ void __launch_bounds__(BATCH_NT, 2) k_batch(const BatchArgs a) {
 
 int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
                       int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars, cudaStream_t st,
-                      std::vector<PassParams>& out, std::vector<char>* tma_ok);
+                      std::vector<PassParams>& out, std::vector<char>* tma_ok, const uint64_t* user_in = nullptr,
+                      int32_t n_user_in = 0, const uint64_t* user_out = nullptr, int32_t n_user_out = 0);
 
 }  // namespace rk
 
@@ -231,7 +232,7 @@ extern "C" int rk_batch_create(rk_fft_plan* const* plans, int32_t nplans, rk_bat
         maxlevel = std::max<int>(maxlevel, (int)p->passes.size());
         for (const PassRec& r : p->passes) {
             int v = 0;
-            if (r.kind != PK_LINE || r.use_tc || !batch_variant(r.dbl, r.L, r.mode, r.var, &v))
+            if (r.kind != PK_LINE || r.use_tc || r.user_bits || !batch_variant(r.dbl, r.L, r.mode, r.var, &v))
                 return fail(RK_ERR_UNSUPPORTED, "rk_batch_create: pass '" + r.note + "' (L=" + std::to_string(r.L) +
                                                      ") has no batched variant");
             smem = std::max(smem, r.li.smem);

@@ -11,8 +11,10 @@
 // twiddle by W_R^(n2*k1), B-point DFTs on contiguous groups, then a register
 // permutation that the compiler resolves to renaming.
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 namespace rk {
 

@@ -89,6 +89,9 @@ struct PassRec {
     void* pair_counters = nullptr; // task counter + per-plane row-tile counters
     int64_t pair_ntasks = 0, pair_planes = 0;
     int32_t pair_a = 0, pair_b = 0;
+    int user_bits = 0;             // 1: loads an RK_FMT_USER input edge, 2: stores one
+    void* user_lib = nullptr;      // cudaLibrary_t of the installed run-time compiled kernel
+    const void* user_kern = nullptr;  // its cudaKernel_t
     bool tma_reencode = false;     // tensor map over the user's input: re-encode per call
     const void* tma_ptr = nullptr; // pointer the current map was encoded for
     int tma_rows = 0;

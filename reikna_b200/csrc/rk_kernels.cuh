@@ -13,8 +13,10 @@
 // sin/cos (reikna/fft/fft.mako:636-649), and transformations applied on the first
 // load and the last store (reikna/core/transformation_modules.py:260-318).
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 #include "rk_dft.cuh"
 #include "rk_params.h"
@@ -230,6 +232,13 @@ __device__ __forceinline__ cplx<T> side_load(const Side& s, const LineAddr& la, 
                     v.x = (T)reinterpret_cast<const double*>(s.ptr)[off];
                     v.y = (T)reinterpret_cast<const double*>(s.ptr2)[off - s.offset + s.offset2];
                     break;
+#ifdef RK_USER_LOAD
+                case RK_FMT_USER:
+                    // transformation code compiled with this kernel: off is the flat
+                    // C-order index of the element in the FFT array
+                    v = RK_USER_LOAD<T>(s, off);
+                    break;
+#endif
                 default:
                     break;
             }
@@ -320,6 +329,11 @@ __device__ __forceinline__ void side_store(const Side& s, const PassParams& p, c
             reinterpret_cast<double*>(s.ptr)[off] = (double)v.x;
             reinterpret_cast<double*>(s.ptr2)[off - s.offset + s.offset2] = (double)v.y;
             break;
+#ifdef RK_USER_STORE
+        case RK_FMT_USER:
+            RK_USER_STORE<T>(s, off, v);
+            break;
+#endif
         default:
             break;
     }
@@ -665,7 +679,9 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
             return pos * NL + ln;
     }
 
-    template <int S, int P>
+    // TWS: the stage twiddle table `tw` is a copy in shared memory (plain loads;
+    // the read-only global path must not address shared memory)
+    template <int S, int P, bool TWS = false>
     static __device__ __forceinline__ void stages(V* v, V* sm, int ln, int tb, const V* tw) {
         if constexpr (S < NS) {
             constexpr int R = RC::R[S];
@@ -683,7 +699,7 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
                     if constexpr (R <= 16) {
                         V w[R - 1];
 #pragma unroll
-                        for (int m = 1; m < R; ++m) w[m - 1] = __ldg(tws + (m - 1) * J + j1);
+                        for (int m = 1; m < R; ++m) w[m - 1] = TWS ? tws[(m - 1) * J + j1] : __ldg(tws + (m - 1) * J + j1);
                         dft<R>(v + z * R);
 #pragma unroll
                         for (int m = 1; m < R; ++m) v[z * R + m] = cmul(v[z * R + m], w[m - 1]);
@@ -691,7 +707,8 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
                         // radix 32: keep the register budget, load after the butterfly
                         dft<R>(v + z * R);
 #pragma unroll
-                        for (int m = 1; m < R; ++m) v[z * R + m] = cmul(v[z * R + m], __ldg(tws + (m - 1) * J + j1));
+                        for (int m = 1; m < R; ++m)
+                            v[z * R + m] = cmul(v[z * R + m], TWS ? tws[(m - 1) * J + j1] : __ldg(tws + (m - 1) * J + j1));
                     }
 #pragma unroll
                     for (int m = 0; m < R; ++m) sm[sidx(ln, l + P * (m + R * j1))] = v[z * R + m];
@@ -704,7 +721,7 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
 #pragma unroll
                     for (int m = 0; m < R2; ++m) v[z * R2 + m] = sm[sidx(ln, tb + TPL * z + (L / R2) * m)];
                 __syncthreads();
-                stages<S + 1, P * R>(v, sm, ln, tb, tw);
+                stages<S + 1, P * R, TWS>(v, sm, ln, tb, tw);
             } else {
 #pragma unroll
                 for (int z = 0; z < NB; ++z) dft<R>(v + z * R);
@@ -714,8 +731,9 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
 
     // v holds stage-0 inputs: v[z*R0 + m] = x[tb + TPL z + (L/R0) m];
     // afterwards v[z*Rl + m] = X[tb + TPL z + (L/Rl) m]
+    template <bool TWS = false>
     static __device__ __forceinline__ void run(V* v, V* sm, int ln, int tb, const V* tw) {
-        stages<0, 1>(v, sm, ln, tb, tw);
+        stages<0, 1, TWS>(v, sm, ln, tb, tw);
     }
 
     static constexpr int R0 = RC::R[0];

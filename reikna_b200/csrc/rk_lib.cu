@@ -239,7 +239,12 @@ static int fmt_is_complex(int f) { return f == RK_FMT_C64 || f == RK_FMT_C128; }
 static int fmt_is_pair(int f) { return f == RK_FMT_F32_PAIR || f == RK_FMT_F64_PAIR; }
 static int fmt_is_real(int f) { return f == RK_FMT_F32 || f == RK_FMT_F64; }
 // arrays a side of this format reads or writes (RK_FMT_CONST / RK_FMT_IGNORE: none)
-static int fmt_arrays(int f) { return fmt_is_pair(f) ? 2 : (f == RK_FMT_CONST || f == RK_FMT_IGNORE) ? 0 : 1; }
+static int fmt_arrays(int f) {
+    return fmt_is_pair(f) ? 2 : (f == RK_FMT_CONST || f == RK_FMT_IGNORE || f == RK_FMT_USER) ? 0 : 1;
+}
+static bool desc_has_user(const rk_fft_desc& d) {
+    return d.input.format == RK_FMT_USER || d.output.format == RK_FMT_USER;
+}
 // an additive term (or a constant input) that only the general element path applies
 static bool edge_has_add(const rk_edge& e) {
     return e.format == RK_FMT_CONST || e.add_slot >= 0 || e.add_re != 0.0 || e.add_im != 0.0;
@@ -337,7 +342,8 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
         set_error("a one-pass real transform needs a transform of the last axis only, of at least 8 points");
         return RK_ERR_UNSUPPORTED;
     }
-    if (real_flags && (edge_has_add(d.input) || edge_has_add(d.output) || d.output.format == RK_FMT_IGNORE)) {
+    if (real_flags && (edge_has_add(d.input) || edge_has_add(d.output) || d.output.format == RK_FMT_IGNORE ||
+                       desc_has_user(d))) {
         set_error("a one-pass real transform takes no additive term, constant input or ignored output");
         return RK_ERR_UNSUPPORTED;
     }
@@ -389,11 +395,14 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
     // the two innermost dims, both transformed powers of two: one clustered pass, or
     // (RK_FLAG_PAIR) a row pass and a column pass run as one plane-ordered launch
     PairInfo pair_probe;
-    const bool want_pair = (d.flags & RK_FLAG_PAIR) && nd >= 2 && axes.size() >= 2 && axes[0] == nd - 1 &&
+    // (an edge read or written by run-time compiled code takes line passes only)
+    const bool want_pair = !desc_has_user(d) && (d.flags & RK_FLAG_PAIR) && nd >= 2 && axes.size() >= 2 &&
+                           axes[0] == nd - 1 &&
                            axes[1] == nd - 2 && is_pow2(d.shape[nd - 1]) && is_pow2(d.shape[nd - 2]) &&
                            pair_info(dbl, (int)d.shape[nd - 1], (int)d.shape[nd - 2], &pair_probe);
     const size_t pair_at = P.passes.size();
-    if (!want_pair && !(d.flags & RK_FLAG_NO_PLANE) && nd >= 2 && axes.size() >= 2 && axes[0] == nd - 1 && axes[1] == nd - 2 &&
+    if (!want_pair && !(d.flags & RK_FLAG_NO_PLANE) && !desc_has_user(d) && nd >= 2 && axes.size() >= 2 &&
+        axes[0] == nd - 1 && axes[1] == nd - 2 &&
         is_pow2(d.shape[nd - 1]) && is_pow2(d.shape[nd - 2])) {
         PlaneInfo pi;
         if (plane_info(dbl, (int)d.shape[nd - 2], (int)d.shape[nd - 1], (d.flags & RK_FLAG_PLANE_WIDE) ? 1 : 0, &pi)) {
@@ -822,7 +831,7 @@ static int validate(const rk_fft_desc* d) {
             }
         }
         const bool special = (e == &d->input && e->format == RK_FMT_CONST) ||
-                             (e == &d->output && e->format == RK_FMT_IGNORE);
+                             (e == &d->output && e->format == RK_FMT_IGNORE) || e->format == RK_FMT_USER;
         if (!(fmt_is_complex(e->format) || fmt_is_real(e->format) || fmt_is_pair(e->format) || special)) {
             set_error("unsupported edge format");
             return RK_ERR_INVALID;
@@ -1160,6 +1169,8 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         r.st_buf = ps.st.buf == SB_IN ? BUF_IN : ps.st.buf == SB_OUT ? BUF_OUT : ps.st.buf;
         r.ld_edge = ps.ld.buf == SB_IN;
         r.st_edge = ps.st.buf == SB_OUT;
+        r.user_bits = (r.ld_edge && desc->input.format == RK_FMT_USER ? 1 : 0) |
+                      (r.st_edge && desc->output.format == RK_FMT_USER ? 2 : 0);
         r.inplace_safe = ps.inplace_safe;
         r.note = ps.note;
         PassParams& pp = r.prm;
@@ -1381,6 +1392,7 @@ int rk_fft_plan_destroy(rk_fft_plan* plan) {
     for (rk::PassRec& r : plan->passes) {
         if (r.pair_tasks) cudaFree(r.pair_tasks);
         if (r.pair_counters) cudaFree(r.pair_counters);
+        if (r.user_lib) cudaLibraryUnload((cudaLibrary_t)r.user_lib);
     }
     delete plan;
     return RK_OK;
@@ -1435,7 +1447,13 @@ namespace rk {
 // single-pass plan.  Shared by rk_fft_execute and the batched launch.
 int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
                       int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars, cudaStream_t st,
-                      std::vector<PassParams>& out, std::vector<char>* tma_ok) {
+                      std::vector<PassParams>& out, std::vector<char>* tma_ok, const uint64_t* user_in,
+                      int32_t n_user_in, const uint64_t* user_out, int32_t n_user_out) {
+    if (n_user_in < 0 || n_user_in > 8 || n_user_out < 0 || n_user_out > 8 || (n_user_in && !user_in) ||
+        (n_user_out && !user_out)) {
+        set_error("user code takes at most 8 words per edge");
+        return RK_ERR_INVALID;
+    }
     if (!plan) { set_error("null plan"); return RK_ERR_INVALID; }
     const rk_fft_desc& d = plan->desc;
     const int need_in = fmt_arrays(d.input.format);
@@ -1530,6 +1548,7 @@ int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs
             }
             p.ld.add_re = add_in[0];
             p.ld.add_im = add_in[1];
+            for (int k = 0; k < n_user_in; ++k) p.ld.user[k] = user_in[k];
             if (d.input.conj) p.ld.flags ^= SF_PRE_CONJ;
         }
         if (r.st_edge) {
@@ -1542,6 +1561,7 @@ int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs
             }
             p.st.add_re = add_out[0];
             p.st.add_im = add_out[1];
+            for (int k = 0; k < n_user_out; ++k) p.st.user[k] = user_out[k];
             if (p.st.flags & SF_NORM) p.st.post_param = order;
         }
         if (inverse) {
@@ -1582,8 +1602,65 @@ int build_call_params(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs
 
 extern "C" {
 
+int rk_fft_plan_pass_info(const rk_fft_plan* plan, int32_t index, int32_t* info, int64_t* smem) {
+    if (!plan || !info || !smem || index < 0 || index >= (int32_t)plan->passes.size()) {
+        set_error("rk_fft_plan_pass_info: bad arguments");
+        return RK_ERR_INVALID;
+    }
+    const PassRec& r = plan->passes[index];
+    info[0] = r.kind;
+    info[1] = r.L;
+    info[2] = r.mode;
+    info[3] = r.var;
+    info[4] = r.dbl;
+    info[5] = r.kind == PK_LINE ? r.li.nt : r.pi.nt;
+    info[6] = r.user_bits;
+    info[7] = r.kind == PK_LINE ? r.li.nl : 0;
+    *smem = (int64_t)(r.kind == PK_LINE ? r.li.smem : r.pi.smem);
+    return RK_OK;
+}
+
+int rk_fft_plan_set_pass_kernel(rk_fft_plan* plan, int32_t index, const void* image, int64_t size, const char* name) {
+    if (!plan || !image || size <= 0 || !name || index < 0 || index >= (int32_t)plan->passes.size()) {
+        set_error("rk_fft_plan_set_pass_kernel: bad arguments");
+        return RK_ERR_INVALID;
+    }
+    PassRec& r = plan->passes[index];
+    if (r.kind != PK_LINE || r.use_tc || r.use_tma || r.pair_first) {
+        set_error("rk_fft_plan_set_pass_kernel: only plain line passes take an installed kernel");
+        return RK_ERR_UNSUPPORTED;
+    }
+    int cur = 0;
+    CK(cudaGetDevice(&cur));
+    if (cur != plan->device) CK(cudaSetDevice(plan->device));
+    cudaLibrary_t lib = nullptr;
+    cudaKernel_t kern = nullptr;
+    cudaError_t e = cudaLibraryLoadData(&lib, image, nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e == cudaSuccess) e = cudaLibraryGetKernel(&kern, lib, name);
+    if (e == cudaSuccess && r.li.smem > 48 * 1024)
+        e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r.li.smem);
+    if (cur != plan->device) cudaSetDevice(cur);
+    if (e != cudaSuccess) {
+        if (lib) cudaLibraryUnload(lib);
+        set_error(std::string("rk_fft_plan_set_pass_kernel: ") + cudaGetErrorString(e));
+        return RK_ERR_CUDA;
+    }
+    if (r.user_lib) cudaLibraryUnload((cudaLibrary_t)r.user_lib);
+    r.user_lib = lib;
+    r.user_kern = (const void*)kern;
+    return RK_OK;
+}
+
 int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
                    int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars, void* stream) {
+    return rk_fft_execute_user(plan, outputs, n_outputs, inputs, n_inputs, inverse, scalars, n_scalars, nullptr, 0,
+                               nullptr, 0, stream);
+}
+
+int rk_fft_execute_user(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, const void* const* inputs,
+                        int32_t n_inputs, int32_t inverse, const double* scalars, int32_t n_scalars,
+                        const uint64_t* user_in, int32_t n_user_in, const uint64_t* user_out, int32_t n_user_out,
+                        void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     if (plan && inverse && (plan->desc.flags & RK_FLAG_REAL_POST)) {
         set_error("a plan with RK_FLAG_REAL_POST runs forward only");
@@ -1596,7 +1673,15 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
     std::vector<PassParams> prm;
     std::vector<char> tma;
     prm.reserve(4);
-    int rc = build_call_params(plan, outputs, n_outputs, inputs, n_inputs, inverse, scalars, n_scalars, st, prm, &tma);
+    if (plan)
+        for (const PassRec& r : plan->passes)
+            if (r.user_bits && !r.user_kern) {
+                set_error("a pass of this plan runs transformation code compiled at run time: install its kernel "
+                          "with rk_fft_plan_set_pass_kernel first");
+                return RK_ERR_INVALID;
+            }
+    int rc = build_call_params(plan, outputs, n_outputs, inputs, n_inputs, inverse, scalars, n_scalars, st, prm, &tma,
+                               user_in, n_user_in, user_out, n_user_out);
     if (rc) return rc;
     const size_t np = plan->passes.size();
     for (size_t i = 0; i < np; ++i) {
@@ -1621,7 +1706,11 @@ int rk_fft_execute(rk_fft_plan* plan, void* const* outputs, int32_t n_outputs, c
             ++i;
             continue;
         }
-        if (r.kind == PK_PLANE)
+        if (r.user_kern) {
+            void* args[1] = {const_cast<PassParams*>(&p)};
+            const unsigned grid = (unsigned)((p.nlines + r.li.nl - 1) / r.li.nl);
+            e = grid ? cudaLaunchKernel(r.user_kern, dim3(grid), dim3(r.li.nt), args, r.li.smem, st) : cudaSuccess;
+        } else if (r.kind == PK_PLANE)
             e = tma[i] ? r.pti.fn(p, r.plane_tma_blocks, st) : r.pi.fn(p, r.nblocks, st);
         else if (r.use_tc)
             e = tc_launch(p, r.nblocks, st);

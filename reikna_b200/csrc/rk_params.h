@@ -1,6 +1,8 @@
 // Launch parameter blocks shared by the host planner and the device kernels.
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <stdint.h>
+#endif
 
 #include "../../include/reikna_b200.h"
 
@@ -54,6 +56,7 @@ struct Side {
     const void* chirp;
     const void* tab;
     const void* win;      // Hann window table (win_len entries, pass precision), or null
+    uint64_t user[8];     // words for run-time compiled edge code (RK_FMT_USER)
 };
 
 // opaque 128-byte CUtensorMap (encoded on the host with cuTensorMapEncodeTiled)

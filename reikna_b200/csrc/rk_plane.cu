@@ -110,11 +110,14 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, PlaneCfg<T, L1, L2
 // cluster barrier; a timed-out copy wait records the status word and the loop
 // carries on (skipping further waits) so no barrier is left unmatched.
 // ------------------------------------------------------------------------------
+
 template <typename T, int L1, int L2, int Q> struct PlaneTmaCfg {
     using C = PlaneCfg<T, L1, L2, Q>;
     static constexpr int A = C::NLR * C::LS2;   // rows (dense) / row exchange (padded)
     static constexpr int B = C::NLC * L1;       // columns
-    static constexpr size_t SMEM = (size_t)(A + B) * C::ESZ + 64;
+    // stage twiddle tables of the row and column lengths, copied to shared memory
+    static constexpr int TW2 = TwLayout<T, L2>::total(), TW1 = TwLayout<T, L1>::total();
+    static constexpr size_t SMEM = (size_t)(A + B + TW2 + TW1) * C::ESZ + 64;
     // resident CTAs per SM: as many as shared memory allows, capped by the plain config
     static constexpr int BY_SMEM = (int)((227 * 1024) / SMEM) > 0 ? (int)((227 * 1024) / SMEM) : 1;
     static constexpr int MINB = BY_SMEM < C::MINB ? BY_SMEM : C::MINB;
@@ -134,9 +137,16 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, (PlaneTmaCfg<T, L1
     // bars[0]: rows of the plane arrived (TMA); bars[1]: column data arrived (st.async
     // bytes from every CTA); bars[2]: every receiver freed its column buffer
     uint64_t* bars = reinterpret_cast<uint64_t*>(bufB + PlaneTmaCfg<T, L1, L2, Q>::B);
-    const V* tw = reinterpret_cast<const V*>(p.tw);
-    const V* tw2 = reinterpret_cast<const V*>(p.tw2);
+    using TC = PlaneTmaCfg<T, L1, L2, Q>;
+    // rows of 256 points on 16 lanes: the warp-local row transform below
+    constexpr bool ROWL = L2 == 256 && Q > 1 && RT == 16 && ER::NS == 2 && ER::R0 == 16 && ER::TPL == 16;
+    V* tw = reinterpret_cast<V*>(bars + 8);
+    V* tw2 = tw + TC::TW2;
     const int tid = threadIdx.x;
+    // the stage twiddles stay in shared memory for the kernel's life (every plane
+    // uses the same ones; loads from there do not wait on L2)
+    for (int i = tid; i < TC::TW2; i += C::NT) tw[i] = reinterpret_cast<const V*>(p.tw)[i];
+    for (int i = tid; i < TC::TW1; i += C::NT) tw2[i] = reinterpret_cast<const V*>(p.tw2)[i];
     const int q = Q > 1 ? (int)cg::this_cluster().block_rank() : 0;
     const int64_t ncl = gridDim.x / Q;
     const int ln = tid / ER::TPL, tb = tid % ER::TPL;
@@ -168,10 +178,15 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, (PlaneTmaCfg<T, L1
         if (healthy) healthy = mbar_wait(&bars[0], pa, p.status);
         pa ^= 1;
         V v[RT];
+        if constexpr (ROWL) {
 #pragma unroll
-        for (int z = 0; z < RT / ER::R0; ++z)
+            for (int m = 0; m < 16; ++m) v[m] = bufA[ln * L2 + tb + 16 * m];
+        } else {
 #pragma unroll
-            for (int m = 0; m < ER::R0; ++m) v[z * ER::R0 + m] = bufA[ln * L2 + ER::in_pos(tb, z, m)];
+            for (int z = 0; z < RT / ER::R0; ++z)
+#pragma unroll
+                for (int m = 0; m < ER::R0; ++m) v[z * ER::R0 + m] = bufA[ln * L2 + ER::in_pos(tb, z, m)];
+        }
         if (p.ld.flags & SF_SCALE) {
             const V c = cmk<V>((T)p.ld.scale_re, (T)p.ld.scale_im);
 #pragma unroll
@@ -181,12 +196,33 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, (PlaneTmaCfg<T, L1
 #pragma unroll
             for (int i = 0; i < RT; ++i) v[i].y = -v[i].y;
         }
-        __syncthreads();
-        ER::run(v, bufA, ln, tb, tw);
-        if constexpr (ER::NS == 1) __syncthreads();
-        if (tid == 0 && !last) {
-            fence_proxy_async_smem();
-            issue(plane + ncl);
+        if constexpr (ROWL) {
+            // the 16 lanes of a row are one half-warp: the row's exchange between its
+            // two radix-16 stages stays inside the warp, in place in the row's own
+            // landing area, position p at p ^ ((p >> 4) & 15) (no bank conflicts for
+            // either order, no block barrier)
+            V* row = bufA + ln * L2;
+            V* rowt = row + 16 * tb;
+            // stage twiddles from shared memory after the butterfly (short latency;
+            // keeps them out of the live registers during the DFT)
+            dft<16>(v);
+#pragma unroll
+            for (int m = 1; m < 16; ++m) v[m] = cmul(v[m], tw[(m - 1) * 16 + tb]);
+            __syncwarp();
+#pragma unroll
+            for (int m = 0; m < 16; ++m) rowt[m ^ tb] = v[m];
+            __syncwarp();
+#pragma unroll
+            for (int m = 0; m < 16; ++m) v[m] = row[16 * m + (tb ^ m)];
+            dft<16>(v);
+        } else {
+            __syncthreads();
+            ER::template run<true>(v, bufA, ln, tb, tw);
+            if constexpr (ER::NS == 1) __syncthreads();
+            if (tid == 0 && !last) {
+                fence_proxy_async_smem();
+                issue(plane + ncl);
+            }
         }
         if constexpr (Q > 1) {
             if (tid == 0) mbar_arrive_expect_tx(&bars[1], COL_BYTES);
@@ -219,7 +255,14 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, (PlaneTmaCfg<T, L1
 #pragma unroll
             for (int m = 0; m < EC::R0; ++m) v[z * EC::R0 + m] = bufB[EC::sidx(lc, EC::in_pos(tc, z, m))];
         __syncthreads();
-        EC::run(v, bufB, lc, tc, tw2);
+        if constexpr (ROWL) {
+            // every warp is past its rows: the next plane's rows may land in A
+            if (tid == 0 && !last) {
+                fence_proxy_async_smem();
+                issue(plane + ncl);
+            }
+        }
+        EC::template run<true>(v, bufB, lc, tc, tw2);
         if constexpr (EC::NS == 1) __syncthreads();
         // the column buffer is free again: tell every sender of the next plane
         if constexpr (Q > 1)
