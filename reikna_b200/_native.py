@@ -30,6 +30,7 @@ FMT_F64_PAIR = 6
 FMT_I32 = 7
 FMT_CONST = 9
 FMT_IGNORE = 10
+FMT_USER = 11
 
 POST_NONE = 0
 POST_NORM = 1
@@ -52,6 +53,9 @@ EXPORTED = (
     "rk_edge_init",
     "rk_fft_plan_create",
     "rk_fft_execute",
+    "rk_fft_execute_user",
+    "rk_fft_plan_pass_info",
+    "rk_fft_plan_set_pass_kernel",
     "rk_fft_plan_destroy",
     "rk_fft_plan_device_bytes",
     "rk_fft_plan_describe",
@@ -176,6 +180,13 @@ def lib() -> ctypes.CDLL:
             vp,
         ]
         L.rk_fft_plan_destroy.argtypes = [vp]
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        L.rk_fft_execute_user.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(vp), ctypes.c_int32,
+                                          ctypes.c_int32, ctypes.POINTER(ctypes.c_double), ctypes.c_int32, u64p,
+                                          ctypes.c_int32, u64p, ctypes.c_int32, vp]
+        L.rk_fft_plan_pass_info.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_int64)]
+        L.rk_fft_plan_set_pass_kernel.argtypes = [vp, ctypes.c_int32, ctypes.c_char_p, ctypes.c_int64, ctypes.c_char_p]
         L.rk_fft_plan_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.rk_fft_plan_describe.argtypes = [
             ctypes.POINTER(FftDesc),
@@ -314,6 +325,39 @@ class Plan:
                 self._h, outs_a, len(outs), ins_a, len(ins), int(inverse), sc, len(scalars), ctypes.c_void_p(stream)
             )
         )
+
+    def execute_user(self, outs, ins, inverse: int = 0, scalars=(), user_in=(), user_out=(), stream: int = 0) -> None:
+        """``execute`` with the words handed to run-time compiled edge code."""
+        outs_a = (ctypes.c_void_p * max(1, len(outs)))(*outs)
+        ins_a = (ctypes.c_void_p * max(1, len(ins)))(*ins)
+        flat = []
+        for s in scalars:
+            c = complex(s)
+            flat += [c.real, c.imag]
+        sc = (ctypes.c_double * max(1, len(flat)))(*flat) if flat else None
+        ui = (ctypes.c_uint64 * max(1, len(user_in)))(*user_in)
+        uo = (ctypes.c_uint64 * max(1, len(user_out)))(*user_out)
+        check(lib().rk_fft_execute_user(self._h, outs_a, len(outs), ins_a, len(ins), int(inverse), sc, len(scalars),
+                                        ui, len(user_in), uo, len(user_out), ctypes.c_void_p(stream)))
+
+    def pass_info(self) -> list[dict]:
+        """Launch shape of every pass (kind, L, mode, variant, complex128, threads, user
+        bits, lines per CTA, shared memory bytes)."""
+        out = []
+        for i in range(self.launches_total):
+            info = (ctypes.c_int32 * 8)()
+            smem = ctypes.c_int64(0)
+            check(lib().rk_fft_plan_pass_info(self._h, i, info, ctypes.byref(smem)))
+            keys = ("kind", "L", "mode", "var", "dbl", "nt", "user", "nl")
+            out.append(dict(zip(keys, list(info)), smem=int(smem.value)))
+        return out
+
+    @property
+    def launches_total(self) -> int:
+        return len(self.describe()["passes"])
+
+    def set_pass_kernel(self, index: int, cubin: bytes, name: str) -> None:
+        check(lib().rk_fft_plan_set_pass_kernel(self._h, int(index), cubin, len(cubin), name.encode()))
 
     def profile(self, max_calls: int) -> None:
         """Record per-pass CUDA events for the next ``max_calls`` executions."""

@@ -116,6 +116,8 @@ class EdgeSpec:
         return self.affine.mul.const if self.affine.mul.is_const else 1.0 + 0j
 
     def fmt(self) -> int:
+        if self.kind == "user":
+            return N.FMT_USER
         if self.kind == "const":
             return N.FMT_CONST
         if self.kind == "ignore":
@@ -468,3 +470,14 @@ def native_edges(ispec: EdgeSpec, ospec: EdgeSpec, scalar_names: list[str]):
         return base + [f(values) for f in extra]
 
     return ein, eout, scalars
+
+
+def user_spec(fft_shape) -> EdgeSpec:
+    """The native side of an edge served by run-time compiled code: the element's
+    flat C-order index in the FFT array is all the code needs."""
+    nd = len(fft_shape)
+    strides, st = [0] * nd, 1
+    for i in range(nd - 1, -1, -1):
+        strides[i] = st
+        st *= fft_shape[i]
+    return EdgeSpec(ndim=nd, kind="user", shape=list(fft_shape), strides=strides, shift=[0] * nd)

@@ -14,7 +14,7 @@ import numpy
 from .. import _native as N
 from ..core.computation import Computation, array_pointer, scalar_value
 from ..core.signature import Annotation, ArrayMetadata, Parameter, Type
-from ._fold import fold_input, fold_output, native_edges
+from ._fold import UserTransformationError, fold_input, fold_output, native_edges, user_spec
 
 
 def _is_complex(dtype) -> bool:
@@ -53,8 +53,21 @@ class FFT(Computation):
         meta = self._meta
         tree = self._tr_tree
         shape = tuple(meta.shape)
-        ispec = fold_input(tree, "input", shape, meta.dtype)
-        ospec = fold_output(tree, "output", shape, meta.dtype)
+        self._user_edges = {}
+        try:
+            ispec = fold_input(tree, "input", shape, meta.dtype)
+        except UserTransformationError:
+            from .user import EdgeCode
+
+            self._user_edges["input"] = EdgeCode(tree, "input", "input", meta)
+            ispec = user_spec(shape)
+        try:
+            ospec = fold_output(tree, "output", shape, meta.dtype)
+        except UserTransformationError:
+            from .user import EdgeCode
+
+            self._user_edges["output"] = EdgeCode(tree, "output", "output", meta)
+            ospec = user_spec(shape)
         leaves = tree.get_leaf_parameters()
         scalar_names = [p.name for p in leaves if p.annotation.is_scalar() and p.name != "inverse"]
         ein, eout, scalars = native_edges(ispec, ospec, scalar_names)
@@ -80,6 +93,9 @@ class FFT(Computation):
         d, ispec, ospec, scalar_names, scalar_list = self.native_descriptor(flags)
         plan = N.Plan(d)
         ann = {p.name: p.annotation for p in self._tr_tree.get_leaf_parameters()}
+        user = dict(self._user_edges)
+        if user:
+            self._install_user_kernels(plan, user)
 
         def bind(args):
             """(output pointers, input pointers, inverse, scalars) of one call."""
@@ -88,12 +104,41 @@ class FFT(Computation):
             scalars = scalar_list({n: scalar_value(args[n]) for n in scalar_names})
             return outs, ins, int(args["inverse"]), scalars
 
-        def runner(stream: int, args):
-            outs, ins, inverse, scalars = bind(args)
-            plan.execute(outs, ins, inverse=inverse, scalars=scalars, stream=stream)
+        if user:
+            uin, uout = user.get("input"), user.get("output")
+
+            def runner(stream: int, args):
+                outs, ins, inverse, scalars = bind(args)
+                wi = uin.words_of(args, array_pointer) if uin else []
+                wo = uout.words_of(args, array_pointer) if uout else []
+                plan.execute_user(outs, ins, inverse=inverse, scalars=scalars, user_in=wi, user_out=wo, stream=stream)
+        else:
+
+            def runner(stream: int, args):
+                outs, ins, inverse, scalars = bind(args)
+                plan.execute(outs, ins, inverse=inverse, scalars=scalars, stream=stream)
 
         runner.launches = plan.launches
         runner.plan = plan
         runner.bind = bind
         runner.flags = flags
         return runner
+
+    def _install_user_kernels(self, plan, user) -> None:
+        """Compile, for every pass that reads or writes an edge given as code, its
+        kernel with that code, and install it in the plan."""
+        from .. import _rtc
+        from .user import kernel_source
+
+        opts = getattr(self, "_compile_options", {})
+        options = list(opts.get("compiler_options", ()))
+        if opts.get("fast_math"):
+            options.append("-use_fast_math")
+        for i, info in enumerate(plan.pass_info()):
+            if not info["user"]:
+                continue
+            edges = ([user["input"]] if info["user"] & 1 else []) + ([user["output"]] if info["user"] & 2 else [])
+            src = kernel_source(edges, "double" if info["dbl"] else "float", info["L"], info["mode"], info["var"],
+                                info["nt"])
+            cubin = _rtc.compile_cubin(src, f"rk_user_pass{i}.cu", options, keep=opts.get("keep", False))
+            plan.set_pass_kernel(i, cubin, "rk_user_pass")

@@ -147,7 +147,7 @@ def test_spectrogram_chain_fold():
     assert list(d.output.shape)[:2] == [13, 513]
 
 
-def test_code_only_transformation_is_not_fusable():
+def test_code_only_transformation_becomes_a_compiled_edge():
     arr = meta((16,))
     t = Transformation(
         [Parameter("output", Annotation(arr, "o")), Parameter("input", Annotation(arr, "i"))],
@@ -155,8 +155,19 @@ def test_code_only_transformation_is_not_fusable():
     )
     fft = FFT(arr)
     fft.parameter.input.connect(t, t.output, x=t.input)
-    with pytest.raises(NotImplementedError):
-        fft.native_descriptor()
+    d, ispec, *_ = fft.native_descriptor()
+    assert d.input.format == N.FMT_USER and ispec.kind == "user" and ispec.arrays == []
+    # a built-in the code chains cannot mix in is refused with a clear message
+    fft2 = FFT(arr)
+    t2 = Transformation(
+        [Parameter("output", Annotation(arr, "o")), Parameter("input", Annotation(arr, "i"))],
+        "${output.store_same}(${input.load_same});",
+    )
+    fft2.parameter.input.connect(t2, t2.output, x=t2.input)
+    w = tr.hanning_window(arr, 16)
+    fft2.parameter.x.connect(w, w.output, y=w.input)
+    with pytest.raises(NotImplementedError, match="chain with transformation code"):
+        fft2.native_descriptor()
 
 
 def test_type_from_value_and_annotation_roles():
