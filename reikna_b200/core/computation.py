@@ -343,7 +343,7 @@ class ComputationPlan:
             buf = torch.empty(nbytes, dtype=torch.uint8, device=self._device)
             from .signature import _torch_dtype_map
 
-            tdt = _torch_dtype_map()[numpy.dtype(meta.dtype)]
+            tdt = {v: k for k, v in _torch_dtype_map().items()}[numpy.dtype(meta.dtype)]
             internal[name] = torch.as_strided(buf.view(tdt), meta.shape, [st // isz for st in meta.strides],
                                               meta.first_element_offset // isz)
         calls = self._calls
