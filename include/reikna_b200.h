@@ -99,6 +99,8 @@ extern "C" {
                                 2L real samples numpy.fft.irfft gives, as L interleaved pairs
                                 (examples/demo_specialized_fft.py:244-331 as one pass);
                                 rk_fft_execute then rejects inverse = 0 */
+#define RK_FLAG_R16 1024      /* 8192-point complex64 fused Bluestein lines with 16 elements a
+                                thread on 512 threads instead of 32 on 256 (tuning) */
 #define RK_FLAG_NO_HALF 512   /* never run a real signal's last-axis transform as the half-length
                                 FFT of its sample pairs (see rk_fft_plan_create) */
 #define RK_FLAG_ANTIPERIODIC 256 /* with RK_FLAG_REAL_POST or RK_FLAG_REAL_PRE: the 2L real

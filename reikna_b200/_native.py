@@ -48,6 +48,7 @@ FLAG_REAL_POST = 64
 FLAG_REAL_PRE = 128
 FLAG_ANTIPERIODIC = 256
 FLAG_NO_HALF = 512
+FLAG_R16 = 1024
 
 EXPORTED = (
     "rk_edge_init",

@@ -38,7 +38,7 @@ from . import _native as N
 MODES = ("calls", "graph", "graph_par", "persistent")
 
 # bumped when the candidate set changes, so that older cached choices are re-tuned
-_TUNE_VERSION = b"2"
+_TUNE_VERSION = b"3"
 
 
 def _cache_path() -> Path:
@@ -196,10 +196,23 @@ class BatchedFFT:
         return _desc_key([c.native_descriptor(0)[0] for c in self.computations])
 
     def candidates(self):
-        """(mode, flags) pairs the autotuner tries."""
-        out = [("calls", 0), ("calls", N.FLAG_NO_TMA), ("graph", 0), ("graph", N.FLAG_NO_TMA)]
+        """(mode, flags) pairs the autotuner tries: the launch mode crossed with the
+        members' kernel-shape choices (``reikna_b200.autotune.candidates``: TMA
+        staging, plane tile shape, Bluestein radix plan / fusion)."""
+        from .autotune import candidates as member_flags
+
+        shapes = [0, N.FLAG_NO_TMA]
+        for c in self.computations:
+            try:
+                for f in member_flags(c):
+                    if f not in shapes and f != N.FLAG_SPLIT_TC:
+                        shapes.append(f)
+            except (N.NativeError, NotImplementedError, ValueError, AttributeError):
+                pass
+        out = [("calls", 0), ("calls", N.FLAG_NO_TMA)]
+        out += [("graph", f) for f in shapes]
         if len(self.computations) > 1:
-            out += [("graph_par", 0), ("graph_par", N.FLAG_NO_TMA)]
+            out += [("graph_par", f) for f in shapes]
         out.append(("persistent", N.FLAG_NO_PLANE))
         return out
 

@@ -12,6 +12,7 @@ torch stream), like reikna's queue-ordered kernel calls.
 
 from __future__ import annotations
 
+import inspect
 import weakref
 from collections.abc import Callable, Iterable
 from typing import Any
@@ -158,6 +159,29 @@ def stream_handle(stream) -> int:
     raise TypeError(f"cannot interpret {stream!r} as a CUDA stream")
 
 
+class ArrayCheck:
+    """The expected torch dtype, shape and element strides of an array parameter, for
+    a cheap per-call check (``array_pointer`` gives the detailed error otherwise)."""
+
+    def __init__(self, annotation):
+        from .signature import _torch_dtype_map
+
+        self.annotation = annotation
+        inv = {v: k for k, v in _torch_dtype_map().items()}
+        self.tdtype = inv.get(numpy.dtype(annotation.dtype))
+        self.shape = tuple(annotation.shape)
+        isz = numpy.dtype(annotation.dtype).itemsize
+        self.strides = tuple(st // isz for st in annotation.strides)
+
+    def __call__(self, arr) -> int:
+        try:
+            if arr.is_cuda and arr.dtype == self.tdtype and arr.shape == self.shape and arr.stride() == self.strides:
+                return arr.data_ptr()
+        except AttributeError:
+            pass
+        return array_pointer(arr, self.annotation)
+
+
 def array_pointer(arr, annotation) -> int:
     """Device pointer of a CUDA array argument after checking it against its annotation."""
     if not (hasattr(arr, "data_ptr") and hasattr(arr, "is_cuda")):
@@ -184,10 +208,37 @@ class ComputationCallable:
         self.signature = Signature(parameters)
         self.parameter = ParameterContainer(self, parameters)
         self._runner = runner
+        # positional calls bind without inspect.Signature.bind (per-call host cost)
+        params = list(self.signature.parameters.values())
+        self._names = [p.name for p in params]
+        self._defaults = [p.default for p in params]
+        self._scalar_dt = [p.annotation.dtype if p.annotation.is_scalar() else None for p in params]
+        self._required = sum(1 for p in params if p.default is inspect.Parameter.empty)
+
+    def _bind_positional(self, args) -> dict | None:
+        n = len(args)
+        if n < self._required or n > len(self._names):
+            return None
+        out = {}
+        for i, name in enumerate(self._names):
+            if i < n:
+                v = args[i]
+                dt = self._scalar_dt[i]
+                if dt is not None:
+                    v = numpy.asarray(v, dtype=dt).flat[0]
+                out[name] = v
+            else:
+                d = self._defaults[i]
+                if d is inspect.Parameter.empty:
+                    return None
+                out[name] = d
+        return out
 
     def __call__(self, stream, *args, **kwds):
-        bound = self.signature.bind_with_defaults(args, kwds, cast=True)
-        return self._runner(stream_handle(stream), bound.arguments)
+        bound = None if kwds else self._bind_positional(args)
+        if bound is None:
+            bound = self.signature.bind_with_defaults(args, kwds, cast=True).arguments
+        return self._runner(stream_handle(stream), bound)
 
     @property
     def launches(self) -> int:

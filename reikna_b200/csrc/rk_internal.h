@@ -111,6 +111,7 @@ struct DeviceTables {
     void* stw_f = nullptr;     // float2 stage twiddle tables, all L (TwLayout)
     void* stw_d = nullptr;     // double2 stage twiddle tables
     int64_t off_f[16] = {0};   // element offset of the table of L = 2^i
+    int64_t off_f_r16 = 0;     // the 16-element plan of L = 8192 (RadixP<float, 8192, 1>)
     int64_t off_d[16] = {0};
     int64_t bytes = 0;
     void* tw4hi_f = nullptr;   // float2[4096]

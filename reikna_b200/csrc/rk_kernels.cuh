@@ -64,12 +64,23 @@ RK_RADIX(double, 4096, 16, 16, 16, 16)
 RK_RADIX(double, 8192, 16, 16, 16, 16, 2)
 #undef RK_RADIX
 
+// Radix plan PL of a length: 0 = the table above; 1 = sixteen elements a thread where
+// the table holds 32 (8192-point float32 lines on 512 threads, the 16-element
+// stages {16, 16, 16, 2}: half the registers a thread, twice the warps a line).
+// Line-pass variant codes carry the plan in bit 4 (VAR = variant + 16 PL).
+template <typename T, int L, int PL = 0> struct RadixP : Radix<T, L> {};
+template <> struct RadixP<float, 8192, 1> {
+    static constexpr int RT = 16;
+    static constexpr int R[] = {16, 16, 16, 2};
+    static constexpr int NS = 4;
+};
+
 // Stage twiddle tables of a length-L line: stage s (radix R, P = product of the
 // earlier radices, J = L / (P R) butterfly groups) needs W_{L/P}^(j1 m) for
 // 1 <= m < R, j1 < J, stored as [m - 1][j1]; the stages follow each other and the
 // last stage needs none.  Generated in FP64 on the device (rk_lib.cu).
-template <typename T, int L> struct TwLayout {
-    using RC = Radix<T, L>;
+template <typename T, int L, int PL = 0> struct TwLayout {
+    using RC = RadixP<T, L, PL>;
     static constexpr int size_of(int s) {
         int P = 1;
         for (int i = 0; i < s; ++i) P *= RC::R[i];
@@ -87,8 +98,8 @@ template <typename T> struct Vec;   // lanes per 128-byte segment
 template <> struct Vec<float> { static constexpr int N = 16; };
 template <> struct Vec<double> { static constexpr int N = 8; };
 
-template <typename T, int L, int MODE> struct LineCfg {
-    using RC = Radix<T, L>;
+template <typename T, int L, int MODE, int PL = 0> struct LineCfg {
+    using RC = RadixP<T, L, PL>;
     static constexpr int RT = RC::RT;
     static constexpr int TPL = L / RT;
     static constexpr int ESZ = 2 * sizeof(T);
@@ -666,10 +677,10 @@ __device__ __forceinline__ void store_block(const Side& s, const PassParams& p, 
 // ------------------------------------------------------------------------------
 // Stockham engine
 // ------------------------------------------------------------------------------
-template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct Engine {
+template <typename T, int L, int MODE, int PL = 0, int NL_ = LineCfg<T, L, MODE, PL>::NL> struct Engine {
     using V = cplx<T>;
-    using Cfg = LineCfg<T, L, MODE>;
-    using RC = Radix<T, L>;
+    using Cfg = LineCfg<T, L, MODE, PL>;
+    using RC = RadixP<T, L, PL>;
     static constexpr int RT = Cfg::RT, TPL = Cfg::TPL, NL = NL_, NS = RC::NS;
 
     static __device__ __forceinline__ int sidx(int ln, int pos) {
@@ -691,12 +702,13 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
                 // [m - 1][j1] (TwLayout; each an FP64 value rounded once), loaded
                 // before the butterfly so their latency overlaps its arithmetic
                 constexpr int J = L / (P * R);
-                const V* tws = tw + TwLayout<T, L>::offset(S);
+                const V* tws = tw + TwLayout<T, L, PL>::offset(S);
 #pragma unroll
                 for (int z = 0; z < NB; ++z) {
                     const int b = tb + TPL * z;
                     const int l = b % P, j1 = b / P;
-                    if constexpr (R <= 16) {
+                    // (plan 1 keeps to half the registers: twiddles after the butterfly)
+                    if constexpr (R <= 16 && PL == 0) {
                         V w[R - 1];
 #pragma unroll
                         for (int m = 1; m < R; ++m) w[m - 1] = TWS ? tws[(m - 1) * J + j1] : __ldg(tws + (m - 1) * J + j1);
@@ -750,11 +762,12 @@ template <typename T, int L, int MODE, int NL_ = LineCfg<T, L, MODE>::NL> struct
 // whose output positions are strided by N1 while consecutive lines are adjacent).
 // One CTA's tile (NL lines starting at line block * NL) of a line pass; shared by
 // the per-pass kernel k_line and the persistent batch kernel (rk_batch.cu).
-template <typename T, int L, int MODE, int VAR>
+template <typename T, int L, int MODE, int VARC>
 __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, unsigned char* smem, int tid) {
+    constexpr int VAR = VARC & 15, PL = VARC >> 4;   // variant, radix plan
     using V = cplx<T>;
-    using E = Engine<T, L, MODE>;
-    using Cfg = LineCfg<T, L, MODE>;
+    using E = Engine<T, L, MODE, PL>;
+    using Cfg = LineCfg<T, L, MODE, PL>;
     constexpr int RT = Cfg::RT, TPL = Cfg::TPL, NL = Cfg::NL;
     constexpr int R0 = E::R0, RL = E::RL;
     V* sm = reinterpret_cast<V*>(smem);
@@ -878,7 +891,7 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
 }
 
 template <typename T, int L, int MODE, int VAR>
-__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassParams p) {
+__global__ void __launch_bounds__(LineCfg<T, L, MODE, (VAR >> 4)>::NT) k_line(const PassParams p) {
     extern __shared__ __align__(16) unsigned char rk_smem[];
     line_body<T, L, MODE, VAR>(p, blockIdx.x, rk_smem, threadIdx.x);
 }
@@ -890,20 +903,21 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line(const PassPara
 // from 59 to 41 us with the paired loads split and the approximate square root.
 // Other bodies keep the register count ptxas picks by itself (any minimum-blocks
 // bound, 1 included, lets it spend registers up to the bound).
-template <typename T, int L, int MODE, int VAR> struct LineMinBlocks {
-    static constexpr int V = (VAR == 1 && Radix<T, L>::RT == 16 && L >= 512 && LineCfg<T, L, MODE>::NT <= 256) ? 2
+template <typename T, int L, int MODE, int VARC> struct LineMinBlocks {
+    static constexpr int VAR = VARC & 15, PL = VARC >> 4;
+    static constexpr int V = (VAR == 1 && RadixP<T, L, PL>::RT == 16 && L >= 512 && LineCfg<T, L, MODE, PL>::NT <= 256) ? 2
                              : (VAR >= 3 && sizeof(T) == 4 && L >= 256 && L <= 1024)                          ? 4
                                                                                                                 : 1;
 };
 
 template <typename T, int L, int MODE, int VAR>
-__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT, 2) k_line_2(const PassParams p) {
+__global__ void __launch_bounds__(LineCfg<T, L, MODE, (VAR >> 4)>::NT, 2) k_line_2(const PassParams p) {
     extern __shared__ __align__(16) unsigned char rk_smem[];
     line_body<T, L, MODE, VAR>(p, blockIdx.x, rk_smem, threadIdx.x);
 }
 
 template <typename T, int L, int MODE, int VAR>
-__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT, 4) k_line_4(const PassParams p) {
+__global__ void __launch_bounds__(LineCfg<T, L, MODE, (VAR >> 4)>::NT, 4) k_line_4(const PassParams p) {
     extern __shared__ __align__(16) unsigned char rk_smem[];
     line_body<T, L, MODE, VAR>(p, blockIdx.x, rk_smem, threadIdx.x);
 }

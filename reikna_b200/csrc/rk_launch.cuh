@@ -6,9 +6,9 @@
 namespace rk {
 
 template <typename T, int L, int MODE, int VAR> struct LineLauncher {
-    using Cfg = LineCfg<T, L, MODE>;
+    using Cfg = LineCfg<T, L, MODE, (VAR >> 4)>;
     static size_t smem() {
-        const bool need = Radix<T, L>::NS > 1 || VAR != 0;
+        const bool need = RadixP<T, L, (VAR >> 4)>::NS > 1 || VAR != 0;
         return need ? (size_t)(MODE == MODE_POS ? Cfg::NL * Cfg::LS : Cfg::NL * L) * Cfg::ESZ : 0;
     }
     static constexpr auto kernel() {

@@ -73,12 +73,12 @@ struct StageSeg {
     int Lp, R, J;
 };
 
-template <typename T, int L> static void stage_segs(std::vector<StageSeg>& segs, int64_t base) {
-    using RC = Radix<T, L>;
+template <typename T, int L, int PL = 0> static void stage_segs(std::vector<StageSeg>& segs, int64_t base) {
+    using RC = RadixP<T, L, PL>;
     int P = 1;
     for (int s = 0; s + 1 < RC::NS; ++s) {
         const int R = RC::R[s];
-        segs.push_back(StageSeg{base + TwLayout<T, L>::offset(s), L / P, R, L / (P * R)});
+        segs.push_back(StageSeg{base + TwLayout<T, L, PL>::offset(s), L / P, R, L / (P * R)});
         P *= R;
     }
 }
@@ -118,6 +118,10 @@ int device_tables(int device, DeviceTables** out) {
     int64_t nf = 0, ndd = 0;
     stage_layout<float, 1, 16384>(sf, t->off_f, nf);
     stage_layout<double, 1, 8192>(sd, t->off_d, ndd);
+    // the 16-element plan of 8192-point float32 lines, after the others
+    t->off_f_r16 = nf;
+    stage_segs<float, 8192, 1>(sf, nf);
+    nf += TwLayout<float, 8192, 1>::total();
     CK(cudaMalloc(&t->stw_f, std::max<int64_t>(nf, 1) * sizeof(float2)));
     CK(cudaMalloc(&t->stw_d, std::max<int64_t>(ndd, 1) * sizeof(double2)));
     CK(cudaMalloc(&t->tw4hi_f, TW4_HALF * sizeof(float2)));
@@ -507,6 +511,9 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
                 PassSpec p;
                 p.L = (int)M; p.var = 1; p.blue_axis = ax;
                 p.mode = I == 1 ? MODE_POS : MODE_LANE;
+                // RK_FLAG_R16: 8192-point float32 lines on the 16-element plan with 512
+                // threads (variant bit 16) instead of 32 elements on 256 threads
+                if (!dbl && M == 8192 && I == 1 && (d.flags & RK_FLAG_R16)) p.var = 1 + 16;
                 p.axis = ax;
                 p.O = O; p.C = 1; p.I = I;
                 p.ld.buf = cur; p.ld.ax_len = n; p.ld.cA = 0; p.ld.jB = 1;
@@ -1162,7 +1169,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         r.dbl = dbl;
         r.L = ps.L;
         r.mode = ps.mode;
-        r.blue = ps.var == 1;
+        r.blue = (ps.var & 15) == 1;
         r.var = ps.var;
         r.axis = ps.axis;
         r.ld_buf = ps.ld.buf == SB_IN ? BUF_IN : ps.ld.buf == SB_OUT ? BUF_OUT : ps.ld.buf;
@@ -1262,7 +1269,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
                 pp.tw = (const double2*)tabs->stw_d + tabs->off_d[lg];
                 pp.tw2 = (const double2*)tabs->stw_d + tabs->off_d[lg2];
             } else {
-                pp.tw = (const float2*)tabs->stw_f + tabs->off_f[lg];
+                pp.tw = (const float2*)tabs->stw_f + ((ps.var >> 4) ? tabs->off_f_r16 : tabs->off_f[lg]);
                 pp.tw2 = (const float2*)tabs->stw_f + tabs->off_f[lg2];
             }
         }

@@ -41,8 +41,8 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, PlaneCfg<T, L1, L2
     k_plane(const PassParams p) {
     using V = cplx<T>;
     using C = PlaneCfg<T, L1, L2, Q>;
-    using ER = Engine<T, L2, MODE_POS, C::NLR>;
-    using EC = Engine<T, L1, MODE_LANE, C::NLC>;
+    using ER = Engine<T, L2, MODE_POS, 0, C::NLR>;
+    using EC = Engine<T, L1, MODE_LANE, 0, C::NLC>;
     constexpr int RT = C::RT;
     extern __shared__ __align__(16) unsigned char rk_smem[];
     V* sm = reinterpret_cast<V*>(rk_smem);
@@ -128,8 +128,8 @@ __global__ void __launch_bounds__(PlaneCfg<T, L1, L2, Q>::NT, (PlaneTmaCfg<T, L1
     k_plane_tma(const __grid_constant__ PassParams p) {
     using V = cplx<T>;
     using C = PlaneCfg<T, L1, L2, Q>;
-    using ER = Engine<T, L2, MODE_POS, C::NLR>;
-    using EC = Engine<T, L1, MODE_LANE, C::NLC>;
+    using ER = Engine<T, L2, MODE_POS, 0, C::NLR>;
+    using EC = Engine<T, L1, MODE_LANE, 0, C::NLC>;
     constexpr int RT = C::RT;
     extern __shared__ __align__(128) unsigned char rk_smem[];
     V* bufA = reinterpret_cast<V*>(rk_smem);

@@ -12,7 +12,7 @@ from __future__ import annotations
 import numpy
 
 from .. import _native as N
-from ..core.computation import Computation, array_pointer, scalar_value
+from ..core.computation import ArrayCheck, Computation, array_pointer, scalar_value
 from ..core.signature import Annotation, ArrayMetadata, Parameter, Type
 from ._fold import UserTransformationError, fold_input, fold_output, native_edges, user_spec
 
@@ -97,11 +97,16 @@ class FFT(Computation):
         if user:
             self._install_user_kernels(plan, user)
 
+        checks = {n: ArrayCheck(ann[n]) for n in list(ospec.arrays) + list(ispec.arrays)}
+        out_checks = [(n, checks[n]) for n in ospec.arrays]
+        in_checks = [(n, checks[n]) for n in ispec.arrays]
+
         def bind(args):
             """(output pointers, input pointers, inverse, scalars) of one call."""
-            outs = [array_pointer(args[n], ann[n]) for n in ospec.arrays]
-            ins = [array_pointer(args[n], ann[n]) for n in ispec.arrays]
-            scalars = scalar_list({n: scalar_value(args[n]) for n in scalar_names})
+            outs = [c(args[n]) for n, c in out_checks]
+            ins = [c(args[n]) for n, c in in_checks]
+            scalars = scalar_list({n: scalar_value(args[n]) for n in scalar_names}) if scalar_names else \
+                scalar_list({})
             return outs, ins, int(args["inverse"]), scalars
 
         if user:
