@@ -808,7 +808,34 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
             load_block<T, RT, half, lp>(p.ld, la, [&](int i) { return E::in_pos(tb, i / R0, i % R0); }, v);
         }
     }
-    E::run(v, sm, ln, tb, tw);
+    // the fused Bluestein pass runs the same line FFT twice: one copy of its code,
+    // looped (half the instruction footprint of two inlined copies)
+    if constexpr (VAR != 1) E::run(v, sm, ln, tb, tw);
+#pragma unroll 1
+    for (int it = 0; it < (VAR == 1 ? 2 : 0); ++it) {
+        E::run(v, sm, ln, tb, tw);
+        if constexpr (VAR == 1) {
+            if (it == 0) {
+                // multiply by the kernel spectrum (1/M folded in) and conjugate, so
+                // that a second forward FFT followed by a conjugation yields the
+                // inverse FFT
+                const V* K = reinterpret_cast<const V*>(p.blue_k);
+#pragma unroll
+                for (int z = 0; z < RT / RL; ++z)
+#pragma unroll
+                    for (int m = 0; m < RL; ++m) {
+                        const int pos = E::out_pos(tb, z, m);
+                        sm[E::sidx(ln, pos)] = cconj(cmul(v[z * RL + m], K[pos]));
+                    }
+                __syncthreads();
+#pragma unroll
+                for (int z = 0; z < RT / R0; ++z)
+#pragma unroll
+                    for (int m = 0; m < R0; ++m) v[z * R0 + m] = sm[E::sidx(ln, E::in_pos(tb, z, m))];
+                __syncthreads();
+            }
+        }
+    }
     if constexpr (VAR == 4) {
         // antiperiodic inverse: W_2L^m on the FFT's output, which the store then
         // conjugates (the inverse's last conjugation) into W_2L^-m on the result
@@ -819,25 +846,6 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
 #pragma unroll
                 for (int m = 0; m < RL; ++m) v[z * RL + m] = cmul(v[z * RL + m], __ldg(tt + E::out_pos(tb, z, m)));
         }
-    }
-    if constexpr (VAR == 1) {
-        // multiply by the kernel spectrum (1/M folded in) and conjugate, so that a
-        // second forward FFT followed by a conjugation yields the inverse FFT
-        const V* K = reinterpret_cast<const V*>(p.blue_k);
-#pragma unroll
-        for (int z = 0; z < RT / RL; ++z)
-#pragma unroll
-            for (int m = 0; m < RL; ++m) {
-                const int pos = E::out_pos(tb, z, m);
-                sm[E::sidx(ln, pos)] = cconj(cmul(v[z * RL + m], K[pos]));
-            }
-        __syncthreads();
-#pragma unroll
-        for (int z = 0; z < RT / R0; ++z)
-#pragma unroll
-            for (int m = 0; m < R0; ++m) v[z * R0 + m] = sm[E::sidx(ln, E::in_pos(tb, z, m))];
-        __syncthreads();
-        E::run(v, sm, ln, tb, tw);
     }
     if constexpr (VAR == 3 || VAR == 5 || VAR == 6) {
         // real-signal spectrum from the half-length spectrum Z of this line (the line
