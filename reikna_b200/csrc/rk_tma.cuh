@@ -11,7 +11,12 @@ template <typename T, int L, int MODE> struct TmaCfg {
     static constexpr int NL = Cfg::NL, NT = Cfg::NT, ESZ = Cfg::ESZ;
     static constexpr int TILE = NL * L;                                           // elements copied
     static constexpr int BUF = MODE == MODE_POS ? NL * Cfg::LS : NL * L;          // elements per buffer
-    static constexpr size_t SMEM = 2 * (size_t)BUF * ESZ + 64;                     // + 2 mbarriers
+    static constexpr size_t SMEM0 = 2 * (size_t)BUF * ESZ + 64;                    // + mbarriers
+    // the stage twiddles move to shared memory when that costs no resident CTA
+    static constexpr int TWN = TwLayout<T, L>::total();
+    static constexpr bool TWS =
+        TWN > 0 && (227 * 1024) / (SMEM0 + (size_t)TWN * ESZ) == (227 * 1024) / SMEM0;
+    static constexpr size_t SMEM = SMEM0 + (TWS ? (size_t)TWN * ESZ : 0);
 };
 
 template <typename T, int L, int MODE>
@@ -24,8 +29,13 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line_tma(const __gr
     V* buf0 = reinterpret_cast<V*>(rk_smem);
     V* buf1 = buf0 + C::BUF;
     uint64_t* bars = reinterpret_cast<uint64_t*>(buf1 + C::BUF);
-    const V* tw = reinterpret_cast<const V*>(p.tw);
     const int tid = threadIdx.x;
+    const V* tw = reinterpret_cast<const V*>(p.tw);
+    if constexpr (C::TWS) {
+        V* tws = reinterpret_cast<V*>(bars + 8);
+        for (int i = tid; i < C::TWN; i += C::NT) tws[i] = tw[i];
+        tw = tws;   // made visible by the barrier after the mbarrier set-up
+    }
     const int ln = MODE == MODE_POS ? tid / TPL : tid % NL;
     const int tb = MODE == MODE_POS ? tid % TPL : tid / NL;
 
@@ -92,7 +102,7 @@ __global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line_tma(const __gr
             for (int i = 0; i < RT; ++i) v[i].y = -v[i].y;
         }
         __syncthreads();  // the tile is in registers: the buffer becomes the exchange area
-        E::run(v, buf, ln, tb, tw);
+        E::template run<C::TWS>(v, buf, ln, tb, tw);
         if constexpr (E::NS == 1) __syncthreads();
         if (tid == 0 && t + 2 * stride < p.ntiles) {
             fence_proxy_async_smem();
