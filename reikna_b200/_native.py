@@ -314,18 +314,26 @@ class Plan:
         return int(b.value)
 
     def execute(self, outs, ins, inverse: int = 0, scalars=(), stream: int = 0) -> None:
-        outs_a = (ctypes.c_void_p * len(outs))(*outs)
-        ins_a = (ctypes.c_void_p * len(ins))(*ins)
-        flat = []
-        for s in scalars:
-            c = complex(s)
-            flat += [c.real, c.imag]
-        sc = (ctypes.c_double * max(1, len(flat)))(*flat) if flat else None
-        check(
-            lib().rk_fft_execute(
-                self._h, outs_a, len(outs), ins_a, len(ins), int(inverse), sc, len(scalars), ctypes.c_void_p(stream)
-            )
-        )
+        # the pointer arrays are kept per plan and refilled (the call path's host cost)
+        arrs = self.__dict__.get("_arrs")
+        if arrs is None or len(arrs[0]) != len(outs) or len(arrs[1]) != len(ins):
+            arrs = self._arrs = ((ctypes.c_void_p * max(1, len(outs)))(), (ctypes.c_void_p * max(1, len(ins)))())
+        outs_a, ins_a = arrs
+        for i, v in enumerate(outs):
+            outs_a[i] = v
+        for i, v in enumerate(ins):
+            ins_a[i] = v
+        sc = None
+        if scalars:
+            flat = []
+            for s in scalars:
+                c = complex(s)
+                flat += [c.real, c.imag]
+            sc = (ctypes.c_double * len(flat))(*flat)
+        rc = lib().rk_fft_execute(self._h, outs_a, len(outs), ins_a, len(ins), int(inverse), sc, len(scalars),
+                                  stream)
+        if rc:
+            check(rc)
 
     def execute_user(self, outs, ins, inverse: int = 0, scalars=(), user_in=(), user_out=(), stream: int = 0) -> None:
         """``execute`` with the words handed to run-time compiled edge code."""

@@ -144,12 +144,19 @@ class Computation:
         return plan.finalize()
 
 
-def stream_handle(stream) -> int:
-    """cudaStream_t of ``stream``: None (current torch stream), torch stream or int."""
+def _current_raw_stream() -> int:
     import torch
 
+    get = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+    if get is not None:
+        return int(get(torch.cuda.current_device()))
+    return torch.cuda.current_stream().cuda_stream
+
+
+def stream_handle(stream) -> int:
+    """cudaStream_t of ``stream``: None (current torch stream), torch stream or int."""
     if stream is None:
-        return torch.cuda.current_stream().cuda_stream
+        return _current_raw_stream()
     if isinstance(stream, int):
         return stream
     if hasattr(stream, "cuda_stream"):
