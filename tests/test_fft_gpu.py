@@ -435,6 +435,32 @@ def test_fftshift_computation(shape_axes, inverse):
     assert numpy.array_equal(t.cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("shape_axes", [((256, 4096), (0, 1)), ((4096, 256), (0,)), ((64, 64, 64), (1, 2)),
+                                        ((64, 62), (1,)), ((33, 64), (0, 1)), ((8, 1, 128), (0, 2))], ids=str)
+@pytest.mark.parametrize("dtype", [numpy.complex64, numpy.complex128])
+@pytest.mark.parametrize("mode", ["out", "inplace", "offset"])
+def test_fftshift_computation_complex(shape_axes, dtype, mode):
+    """Complex elements take the row form's vector accesses where rows, shifts and
+    addresses allow; a view starting one element into its allocation does not."""
+    from reikna_b200.fft import FFTShift
+
+    torch = _torch()
+    shape, axes = shape_axes
+    rng = numpy.random.default_rng(math.prod(shape))
+    data = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dtype)
+    if mode == "offset":
+        base = torch.zeros(math.prod(shape) + 1, dtype=torch.complex64 if dtype == numpy.complex64 else torch.complex128,
+                           device="cuda")
+        t = base[1:].view(shape)
+        t.copy_(torch.from_numpy(data))
+    else:
+        t = to_dev(data)
+    out = t if mode == "inplace" else torch.empty_like(t)
+    FFTShift(t, axes=axes).compile()(None, out, t)
+    torch.cuda.synchronize()
+    assert numpy.array_equal(out.cpu().numpy(), numpy.fft.fftshift(data, axes=axes))
+
+
 def test_fftshift_unordered_and_no_axes():
     from reikna_b200.fft import FFTShift
 
