@@ -99,6 +99,9 @@ extern "C" {
                                 2L real samples numpy.fft.irfft gives, as L interleaved pairs
                                 (examples/demo_specialized_fft.py:244-331 as one pass);
                                 rk_fft_execute then rejects inverse = 0 */
+#define RK_FLAG_BATCHABLE 2048 /* plan only passes the persistent batched kernel has tile bodies for
+                                (no plane pass, strided fused Bluestein lines of at most 1024
+                                points); rk_batch_create members */
 #define RK_FLAG_R16 1024      /* 8192-point complex64 fused Bluestein lines with 16 elements a
                                 thread on 512 threads instead of 32 on 256 (tuning) */
 #define RK_FLAG_NO_HALF 512   /* never run a real signal's last-axis transform as the half-length

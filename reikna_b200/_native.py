@@ -49,6 +49,7 @@ FLAG_REAL_PRE = 128
 FLAG_ANTIPERIODIC = 256
 FLAG_NO_HALF = 512
 FLAG_R16 = 1024
+FLAG_BATCHABLE = 2048
 
 EXPORTED = (
     "rk_edge_init",

@@ -166,7 +166,7 @@ class BatchedFFT:
     :param device: torch device (default: the current CUDA device).
     :param mode: ``"calls"``, ``"graph"``, ``"graph_par"``, ``"persistent"`` or ``"auto"``.
     :param flags: plan flags for a fixed mode (``"persistent"`` adds
-        ``FLAG_NO_PLANE``, since plane passes have no batched variant).
+        ``FLAG_BATCHABLE``: only passes with a batched tile body).
 
     Call as ``batched(stream, [args_0, args_1, ...])`` where ``args_i`` is the
     positional tuple (or keyword dict) member i's compiled callable takes.
@@ -189,7 +189,7 @@ class BatchedFFT:
         self._variant = None
         self.tuning = None
         if mode != "auto":
-            f = flags | (N.FLAG_NO_PLANE if mode == "persistent" else 0)
+            f = flags | (N.FLAG_BATCHABLE if mode == "persistent" else 0)
             self._variant = _Variant(self.computations, self.device, mode, f)
 
     def key(self) -> str:
@@ -213,7 +213,7 @@ class BatchedFFT:
         out += [("graph", f) for f in shapes]
         if len(self.computations) > 1:
             out += [("graph_par", f) for f in shapes]
-        out.append(("persistent", N.FLAG_NO_PLANE))
+        out.append(("persistent", N.FLAG_BATCHABLE))
         return out
 
     @property

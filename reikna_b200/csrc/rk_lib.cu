@@ -405,7 +405,8 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
                            axes[1] == nd - 2 && is_pow2(d.shape[nd - 1]) && is_pow2(d.shape[nd - 2]) &&
                            pair_info(dbl, (int)d.shape[nd - 1], (int)d.shape[nd - 2], &pair_probe);
     const size_t pair_at = P.passes.size();
-    if (!want_pair && !(d.flags & RK_FLAG_NO_PLANE) && !desc_has_user(d) && nd >= 2 && axes.size() >= 2 &&
+    if (!want_pair && !(d.flags & (RK_FLAG_NO_PLANE | RK_FLAG_BATCHABLE)) && !desc_has_user(d) && nd >= 2 &&
+        axes.size() >= 2 &&
         axes[0] == nd - 1 && axes[1] == nd - 2 &&
         is_pow2(d.shape[nd - 1]) && is_pow2(d.shape[nd - 2])) {
         PlaneInfo pi;
@@ -507,7 +508,10 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
         } else {
             const int64_t M = 2 * bpow2(n);
             P.blue.push_back(BlueAxis{ax, n, M});
-            if ((I == 1 && M <= PM) || (I > 1 && M <= LM)) {
+            // a strided (lane-mode) fused Bluestein line holds up to 2048 complex64
+            // points (four adjacent lines a CTA): one pass instead of four
+            const int64_t blue_lane_max = (dbl || (d.flags & RK_FLAG_BATCHABLE)) ? LM : 2048;
+            if ((I == 1 && M <= PM) || (I > 1 && M <= blue_lane_max)) {
                 PassSpec p;
                 p.L = (int)M; p.var = 1; p.blue_axis = ax;
                 p.mode = I == 1 ? MODE_POS : MODE_LANE;
