@@ -975,6 +975,13 @@ def measure_batch(dev, steps: int, warmup: int, modes=("calls", "graph", "graph_
             cc(None, o, i)
 
     res = {"plain_per_call": {"us": timed(plain, reps) * 1e3}}
+    # each member alone: the batch cannot finish before its longest member, so
+    # plain / max(member) bounds any batching speed-up
+    alone = []
+    for cc, (o, i) in zip(singles, args_list):
+        alone.append(timed(lambda cc=cc, o=o, i=i: cc(None, o, i), reps) * 1e3)
+    res["plain_per_call"]["members_alone_us"] = alone
+    res["plain_per_call"]["max_speedup_bound"] = res["plain_per_call"]["us"] / max(alone)
     plain()
     torch.cuda.synchronize(dev)
     res["plain_per_call"]["rel_l2_vs_fp64"] = [
