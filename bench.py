@@ -72,13 +72,14 @@ def peaks() -> tuple[float, str]:
 
 
 def traffic_from_profiles(kernel_note: str):
-    """DRAM bytes per launch recorded by an ncu capture summary under profiles/."""
+    """DRAM bytes per launch recorded by an ncu capture summary under profiles/ (copied
+    from that capture, not measured in this run); returns (bytes, file) or (None, None)."""
     for f in sorted((ROOT / "profiles").glob("*.md")) + sorted((ROOT / "profiles").glob("*.txt")):
         txt = f.read_text(errors="replace")
         m = re.search(rf"traffic\[{re.escape(kernel_note)}\]\s*=\s*([0-9.eE+]+)", txt)
         if m:
-            return float(m.group(1))
-    return None
+            return float(m.group(1)), f"profiles/{f.name}"
+    return None, None
 
 
 class Clocks:
@@ -417,7 +418,7 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
     dom = max(range(len(per_launch)), key=lambda i: per_launch[i])
     dom_bytes = 2 * ARRAY_BYTES  # each pass reads and writes the whole array once
     achieved = dom_bytes / (per_launch[dom] / 1e3) / 1e9
-    traffic = traffic_from_profiles(passes[dom]["note"] + f"/L{passes[dom]['L']}/{passes[dom]['mode']}")
+    traffic, traffic_src = traffic_from_profiles(passes[dom]["note"] + f"/L{passes[dom]['L']}/{passes[dom]['mode']}")
     line = {
         "metric": METRIC,
         "value": value,
@@ -439,6 +440,8 @@ def run_own(args, rank: int, world: int, local_rank: int) -> int:
             "unit": "GB/s",
             "frac": achieved / peak,
             "traffic": traffic,
+            "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, copied from {traffic_src}"
+            if traffic_src else None,
             "kernel": passes[dom]["note"] + f" L={passes[dom]['L']} {passes[dom]['mode']}",
             "bytes_per_launch_algorithmic": dom_bytes,
             "ms_per_launch": per_launch[dom],

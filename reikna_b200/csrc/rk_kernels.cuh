@@ -863,7 +863,10 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
         const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
         if (tb == 0 && la.ok && p.rnyq) store_nyquist<T>(p.st, la.base + (int64_t)L * p.st.ax_stride, nyq);
         if constexpr (VAR == 3 || VAR == 6) {
-            store_block<T, RT>(p.st, p, la, [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
+            // real-spectrum stores are complex bins or real magnitudes along the line:
+            // the lean paths for those two only (others take the element path)
+            store_block<T, RT, STORE_FAST | STORE_FASTR>(p.st, p, la,
+                                                         [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
         } else {
             __syncthreads();
 #pragma unroll
@@ -875,7 +878,7 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
             const LineAddr ls = line_addr(p.st, sline, p.C, p.I, sline < p.nlines);
 #pragma unroll
             for (int q = 0; q < RT; ++q) v[q] = sm[E::sidx(lane, p0 + TPL * q)];
-            store_block<T, RT>(p.st, p, ls, [&](int q) { return p0 + TPL * q; }, v);
+            store_block<T, RT, STORE_FAST | STORE_FASTR>(p.st, p, ls, [&](int q) { return p0 + TPL * q; }, v);
         }
     } else if constexpr (VAR == 2) {
         static_assert(MODE == MODE_POS, "transposed store needs position mode");
