@@ -103,9 +103,11 @@ int pair_setup(PassRec& ra, PassRec& rb, const PairInfo& pi);
 cudaError_t pair_launch(const PassRec& ra, const PassParams& pa, const PassParams& pb, int32_t* status,
                         cudaStream_t st);
 
-// tensor-core split-precision pass (rk_tc.cu): 1024-point complex64 contiguous lines
+// tensor-core split-precision pass (rk_tc.cu): 256- and 1024-point complex64
+// contiguous lines; tc_prepare generates its tables on the current device (once)
 bool tc_eligible(const PassRec& r);
-cudaError_t tc_launch(const PassParams& p, int64_t nblocks, cudaStream_t st);
+cudaError_t tc_prepare();
+cudaError_t tc_launch(const PassParams& p, int L, cudaStream_t st);
 
 struct DeviceTables {
     void* stw_f = nullptr;     // float2 stage twiddle tables, all L (TwLayout)

@@ -1319,6 +1319,11 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
             r.li = li;
             if (!(desc->flags & RK_FLAG_NO_TMA) && ps.var == 0) setup_tma(r, dbl, nsm);
             if ((desc->flags & RK_FLAG_SPLIT_TC) && tc_eligible(r)) {
+                const cudaError_t te = tc_prepare();
+                if (te != cudaSuccess) {
+                    set_error(std::string("tensor-core tables: ") + cudaGetErrorString(te));
+                    return fail(RK_ERR_CUDA);
+                }
                 r.use_tc = true;
                 r.use_tma = false;
             }
@@ -1724,7 +1729,7 @@ int rk_fft_execute_user(rk_fft_plan* plan, void* const* outputs, int32_t n_outpu
         } else if (r.kind == PK_PLANE)
             e = tma[i] ? r.pti.fn(p, r.plane_tma_blocks, st) : r.pi.fn(p, r.nblocks, st);
         else if (r.use_tc)
-            e = tc_launch(p, r.nblocks, st);
+            e = tc_launch(p, r.L, st);
         else
             e = tma[i] ? r.ti.fn(p, r.nblocks, st) : r.li.fn(p, (p.nlines + r.li.nl - 1) / r.li.nl, st);
         if (e != cudaSuccess) {

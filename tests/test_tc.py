@@ -1,7 +1,9 @@
 """Tensor-core split-precision mode (RK_FLAG_SPLIT_TC) against numpy in FP64.
 
-The mode's error is reported separately from the FP32 path; the test holds it to the
-same bound as complex64 (rel-L2 <= 2e-6 log2 N) and prints both errors.
+The mode runs 256- and 1024-point contiguous complex64 lines on the tensor cores. Its
+error is reported separately from the FP32 path; the tests hold it to the same bound
+as complex64 (rel-L2 <= 2e-6 log2 N), the full-size cases to 4e-7 as well, and print
+both errors.
 """
 
 import numpy
@@ -45,6 +47,57 @@ def test_split_tc_matches_fp64(rows):
     y32, _ = _run(x, 0)
     print(f"rows={rows}: split-TC rel-L2 {err:.3e}, FP32 {rel_l2(y32, ref):.3e}")
     assert err < fft_bound(numpy.complex64, 1024)
+    if rows == 16384:
+        assert err < 4e-7
+
+
+@pytest.mark.parametrize("rows", [1, 7, 64, 65536])
+def test_split_tc_256_matches_fp64(rows):
+    from reikna_b200 import _native as N
+
+    rng = numpy.random.default_rng(70)
+    x = normal_array(rng, (rows, 256), numpy.complex64)
+    ref = numpy.fft.fft(x.astype(numpy.complex128), axis=1)
+    y, ntc = _run(x, N.FLAG_SPLIT_TC)
+    assert ntc == 1
+    err = rel_l2(y, ref)
+    print(f"256 rows={rows}: split-TC rel-L2 {err:.3e}")
+    assert err < fft_bound(numpy.complex64, 256)
+    if rows == 65536:
+        assert err < 4e-7
+    yi, _ = _run(x, N.FLAG_SPLIT_TC, inverse=1, inplace=True)
+    assert rel_l2(yi, numpy.fft.ifft(x.astype(numpy.complex128), axis=1)) < fft_bound(numpy.complex64, 256)
+
+
+@pytest.mark.parametrize("n", [256, 1024])
+@pytest.mark.parametrize("conj_in,conj_out,inverse", [(1, 0, 0), (0, 1, 0), (1, 0, 1), (0, 1, 1), (1, 1, 0)])
+def test_split_tc_edge_conjugation(n, conj_in, conj_out, inverse):
+    """Conjugating edges: one side alone conjugates data in the kernel, both sides of
+    a forward transform (or neither of an inverse) take the conjugate tables."""
+    import torch
+
+    from reikna_b200 import _native as N
+
+    rows = 9
+    x = normal_array(numpy.random.default_rng(71 + n), (rows, n), numpy.complex64)
+    d = N.desc(N.FMT_C64, (rows, n), (1,), N.FLAG_SPLIT_TC)
+    d.input = N.edge(N.FMT_C64, (rows, n))
+    d.output = N.edge(N.FMT_C64, (rows, n))
+    d.input.conj = conj_in
+    d.output.conj = conj_out
+    plan = N.Plan(d)
+    assert plan.tc_passes == 1
+    a = torch.from_numpy(x).cuda()
+    b = torch.empty_like(a)
+    plan.execute([b.data_ptr()], [a.data_ptr()], inverse=inverse, stream=0)
+    torch.cuda.synchronize()
+    xr = x.astype(numpy.complex128)
+    if conj_in:
+        xr = numpy.conj(xr)
+    ref = numpy.fft.ifft(xr, axis=1) if inverse else numpy.fft.fft(xr, axis=1)
+    if conj_out:
+        ref = numpy.conj(ref)
+    assert rel_l2(b.cpu().numpy(), ref) < fft_bound(numpy.complex64, n)
 
 
 @pytest.mark.parametrize("rows", [512, 16384])
@@ -91,7 +144,7 @@ def test_split_tc_request_falls_back_where_not_applicable():
     from reikna_b200 import _native as N
 
     rng = numpy.random.default_rng(13)
-    for shape, axis in (((64, 512), 1), ((1024, 8), 0)):
+    for shape, axis in (((64, 512), 1), ((1024, 8), 0), ((256, 64), 0)):
         x = normal_array(rng, shape, numpy.complex64)
         import torch
 
@@ -113,7 +166,7 @@ def test_split_tc_device_status_clean():
 
 
 def test_split_tc_view_off_the_16_byte_grid():
-    # a view starting 8 bytes into its allocation takes plain loads instead of bulk copies
+    # a view starting 8 bytes into its allocation takes 8-byte loads instead of 16-byte ones
     import torch
 
     from reikna_b200 import _native as N
@@ -123,6 +176,7 @@ def test_split_tc_view_off_the_16_byte_grid():
     x = normal_array(rng, (5, 1024), numpy.complex64)
     base = torch.zeros(5 * 1024 + 1, dtype=torch.complex64, device="cuda")
     view = base[1:].view(5, 1024)
+    assert view.data_ptr() % 16 == 8
     view.copy_(torch.from_numpy(x))
     out = torch.empty_like(view)
     c = FFT(view, axes=(1,)).compile(flags=N.FLAG_SPLIT_TC)
