@@ -294,7 +294,6 @@ __global__ void __launch_bounds__(256, TcCfg<R>::MINB)
             put_split<R>(sm, a_off<R>(row, c0 + 4 * c), re[0], re[1], re[2], re[3]);
             put_split<R>(sm, a_off<R>(row, R + c0 + 4 * c), im[0], im[1], im[2], im[3]);
         }
-        if (tile + gridDim.x < ntiles) load(tile + gridDim.x);
         fence_proxy_async_smem();
         tc_fence_before();
         // every thread leaves together when any wait ran out
@@ -321,6 +320,9 @@ __global__ void __launch_bounds__(256, TcCfg<R>::MINB)
         tc_fence_before();
         if (!__syncthreads_and(ok)) break;
         issue();
+        // the next tile's input: issued here, after the last proxy fence of this tile
+        // (the fence would wait for loads in flight), used by the next stage 1
+        if (tile + gridDim.x < ntiles) load(tile + gridDim.x);
         ok = mbar_wait(bar, phase, p.status);
         phase ^= 1;
         tc_fence_after();
@@ -426,12 +428,18 @@ cudaError_t launch_tc(const PassParams& p, int dir, int xconj, cudaStream_t st) 
             e = cudaFuncSetAttribute(k_tc<R>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared);
             if (e != cudaSuccess) return e;
-            int per_sm = 0, nsm = 0;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc<R>, C::NT, C::SMEM);
+            // resident CTAs an SM: shared memory (1 KB reserved a CTA), registers (a
+            // warp's allocation rounded to 256), threads, and the SM's 512 tensor-memory
+            // columns (2R a CTA); the occupancy query reports one CTA where two fit
+            cudaFuncAttributes fa;
+            e = cudaFuncGetAttributes(&fa, k_tc<R>);
             if (e != cudaSuccess) return e;
+            int nsm = 0, smem_sm = 0;
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            // every resident CTA holds 2R of the SM's 512 tensor-memory columns
-            per_sm = std::max(1, std::min(per_sm, 512 / C::K));
+            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+            const int warp_regs = ((fa.numRegs * 32 + 255) / 256) * 256;
+            const int per_sm = std::max(1, std::min({smem_sm / (C::SMEM + 1024), 65536 / (warp_regs * (C::NT / 32)),
+                                                     2048 / C::NT, 512 / C::K}));
             grid = grid_by_dev[dev] = per_sm * nsm;
         }
     }
