@@ -1134,7 +1134,7 @@ def run_precision(args, rank: int, world: int, local_rank: int) -> int:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f16x2-split/f32-acc",
+        "dtype": "tf32x2-split/f32-acc",
         "data": "synthetic",
         "config": {"workload": "precision_16384x1024_complex64", "shape": list(shape), "axes": [1],
                    "bytes_per_step_algorithmic": b_alg, "l2": "inputs larger than L2, two buffer sets alternate",

@@ -80,8 +80,9 @@ extern "C" {
 /* plan flags */
 #define RK_FLAG_NO_PLANE 1   /* never fuse two axes into one clustered pass */
 #define RK_FLAG_NO_BLUE1 2   /* never use the single-pass Bluestein kernel */
-#define RK_FLAG_SPLIT_TC 4   /* tensor-core split-precision radix-16 stages (1024-point
-                                contiguous complex64 line passes; others run as usual) */
+#define RK_FLAG_SPLIT_TC 4   /* tensor-core split-precision stages (tf32 hi/lo, FP32
+                                accumulate) for 256- and 1024-point contiguous complex64
+                                line passes; others run as usual */
 #define RK_FLAG_PLANE_WIDE 8 /* plane pass on twice as many CTAs per cluster (tuning) */
 #define RK_FLAG_NO_TMA 16    /* never use the persistent TMA-fed line passes */
 #define RK_FLAG_PAIR 32      /* two innermost power-of-two axes: row and column passes in one
