@@ -9,8 +9,8 @@
 // columns are the R real parts then the R imaginary parts; B is the real form of the
 // R-point DFT matrix (N = 2R output reals).
 //
-// Stage 1: row m = (line l, n2) is the vector over n1.  Two threads share a row (one
-// tensor-memory lane, halves of its columns): they load its elements (a warp reads 32
+// Stage 1: row m = (line l, n2) is the vector over n1.  Two or four threads share a row
+// (one tensor-memory lane, parts of its columns): they load its elements (a warp reads 32
 // consecutive n2 of one n1), write them as 16-byte K-major operand rows, read the
 // accumulator back (tcgen05.ld), multiply by W_L^(n2 k1) and write the values as column
 // n2 of the stage-2 rows (l, k1); the operand's padded strides keep those column stores
@@ -26,8 +26,8 @@
 // and rounded once; the twiddle multiply runs in FP32 on the CUDA cores.  The inverse
 // transform uses the conjugate tables instead of conjugating data.
 //
-// The grid is persistent, two (R = 32) or four (R = 16) CTAs of 256 threads an SM; a
-// thread prefetches the next tile's input into registers while the current tile is
+// The grid is persistent: two CTAs of 512 threads an SM (R = 32, four threads a row)
+// or four of 256 (R = 16, two a row); a thread prefetches the next tile's input into registers while the current tile is
 // on the tensor cores.  Tensor memory (2R columns) is allocated once a CTA and freed
 // before exit, also after a timed-out wait; every wait is clock-bounded.
 #include <cuda_runtime.h>
@@ -43,14 +43,14 @@ namespace rk {
 
 namespace {
 
-template <int R>
+template <int R, int TPR = 2>
 struct TcCfg {
     static constexpr int L = R * R;
     static constexpr int ROWS = 128;         // rows of a product = tensor-memory lanes
-    static constexpr int NT = 256;           // two threads a row (column halves)
+    static constexpr int NT = 32 * 4 * TPR;  // TPR threads a row (parts of its columns)
     static constexpr int LINES = ROWS / R;   // lines a tile
     static constexpr int K = 2 * R;          // reals a vector (and output reals)
-    static constexpr int H = R / 2;          // complex values a thread holds of a row
+    static constexpr int H = R / TPR;        // complex values a thread holds of a row
     // A operand, K-major, no swizzle: core matrices of 8 rows x 4 K (16 bytes),
     // K-adjacent core matrices A_LBO apart, 8-row groups A_SBO apart.  A_LBO = 144
     // (not 128) spreads the eight 16-byte chunks of one row over all 32 banks (the
@@ -70,7 +70,8 @@ struct TcCfg {
     static constexpr int OFF_TW = OFF_TAB + 2 * B_BYTES;
     static constexpr int OFF_BAR = OFF_TAB + TAB_BYTES;
     static constexpr int SMEM = OFF_BAR + 16;
-    static constexpr int MINB = R == 32 ? 2 : 4;
+    static constexpr int MINB = TPR == 4 ? 2 : (R == 32 ? 2 : 4);
+    static_assert(H % 4 == 0, "a thread's part of a row is whole 16-byte operand chunks");
     // instruction descriptor: D f32, A and B tf32, both K-major, N = 2R, M = 128
     static constexpr uint32_t IDESC =
         (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(K >> 3) << 17) | ((128u >> 4) << 24);
@@ -152,8 +153,8 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// N consecutive accumulator columns of this thread's lane into r (N = 8 or 16); the
-// registers hold the values only after tcgen05.wait::ld
+// N consecutive accumulator columns of this thread's lane into r (N = 4, 8 or 16);
+// the registers hold the values only after tcgen05.wait::ld
 template <int N>
 __device__ __forceinline__ void tc_ldn(uint32_t taddr, uint32_t* r) {
     if constexpr (N == 16) {
@@ -164,21 +165,25 @@ __device__ __forceinline__ void tc_ldn(uint32_t taddr, uint32_t* r) {
               "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
             : "r"(taddr)
             : "memory");
-    } else {
-        static_assert(N == 8, "8 or 16 columns");
+    } else if constexpr (N == 8) {
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
                        "=r"(r[7])
                      : "r"(taddr)
                      : "memory");
+    } else {
+        static_assert(N == 4, "4, 8 or 16 columns");
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                     : "r"(taddr)
+                     : "memory");
     }
 }
 
-// this thread's half of its accumulator row: columns [c0, c0 + H) (real parts) and
+// this thread's part of its accumulator row: columns [c0, c0 + H) (real parts) and
 // [R + c0, R + c0 + H) (imaginary parts), read only after the wait
-template <int R>
-__device__ __forceinline__ void tc_ld_half(uint32_t taddr, int c0, float* re, float* im) {
-    constexpr int H = R / 2;
+template <int R, int H>
+__device__ __forceinline__ void tc_ld_part(uint32_t taddr, int c0, float* re, float* im) {
     uint32_t a[H], b[H];
     tc_ldn<H>(taddr + c0, a);
     tc_ldn<H>(taddr + R + c0, b);
@@ -196,15 +201,16 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
 
 // xconj bit 0: conjugate the input, bit 1: the output (only when exactly one side
 // conjugates; both together run the inverse tables)
-template <int R>
-__global__ void __launch_bounds__(256, TcCfg<R>::MINB)
+template <int R, int TPR>
+__global__ void __launch_bounds__(TcCfg<R, TPR>::NT, TcCfg<R, TPR>::MINB)
     k_tc(const __grid_constant__ PassParams p, int dir, int xconj) {
-    using C = TcCfg<R>;
+    using C = TcCfg<R, TPR>;
     constexpr int L = C::L, H = C::H;
     extern __shared__ __align__(1024) unsigned char sm[];
     const int t = threadIdx.x, warp = t >> 5;
-    // this thread's row (= tensor-memory lane) and column half
-    const int row = (warp & 3) * 32 + (t & 31), half = warp >> 2, c0 = half * H;
+    // this thread's row (= tensor-memory lane: warp w reaches lanes 32 (w mod 4) ..)
+    // and its part of the row's columns
+    const int row = (warp & 3) * 32 + (t & 31), c0 = (warp >> 2) * H;
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + C::OFF_BAR);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + C::OFF_BAR + 8);
     const uint32_t sbase = smem_u32(sm);
@@ -241,14 +247,23 @@ __global__ void __launch_bounds__(256, TcCfg<R>::MINB)
     const int64_t ntiles = (nlines + C::LINES - 1) / C::LINES;
     const int l = row / R, rr = row % R;   // stage 1: rr = n2; stage 2: rr = k1
 
+    // operand offsets as a thread base plus compile-time steps (l R + c0 is a multiple
+    // of 8, or of 4 with H = 4, so row l R + c0 + i stays in the base's 8-row group
+    // for i < 8 and H = 4 alike; c0 is a multiple of 4): stage 1 writes row `row`, columns c0 + 4c (real) and
+    // R + c0 + 4c (imaginary); stage 2 writes rows l R + c0 + i, columns rr and R + rr
+    constexpr uint32_t IM = (uint32_t)(R / 4) * C::A_LBO;  // column k -> k + R
+    const uint32_t base1 = a_off<R>(row, c0);
+    const uint32_t base2 = a_off<R>(l * R + c0, rr);
+    auto step2 = [](int i) -> uint32_t { return (uint32_t)((i >> 3) * C::A_SBO + (i & 7) * 16); };
+
     // stage-1 input of this thread: x[l][R n1 + n2], n1 = c0 .. c0 + H - 1
     float2 x[H];
     auto load = [&](int64_t tile) {
         const int64_t line = tile * C::LINES + l;
         const bool in = line < nlines;
-        const float2* s = src + line * L + rr;
+        const float2* s = src + line * L + rr + R * c0;
 #pragma unroll
-        for (int i = 0; i < H; ++i) x[i] = in ? s[R * (c0 + i)] : make_float2(0.f, 0.f);
+        for (int i = 0; i < H; ++i) x[i] = in ? s[R * i] : make_float2(0.f, 0.f);
     };
 
     // MMA of one stage: every thread's operand stores are visible to the tensor core,
@@ -291,8 +306,8 @@ __global__ void __launch_bounds__(256, TcCfg<R>::MINB)
                 re[i] = u.x;
                 im[i] = u.y;
             }
-            put_split<R>(sm, a_off<R>(row, c0 + 4 * c), re[0], re[1], re[2], re[3]);
-            put_split<R>(sm, a_off<R>(row, R + c0 + 4 * c), im[0], im[1], im[2], im[3]);
+            put_split<R>(sm, base1 + c * C::A_LBO, re[0], re[1], re[2], re[3]);
+            put_split<R>(sm, base1 + c * C::A_LBO + IM, im[0], im[1], im[2], im[3]);
         }
         fence_proxy_async_smem();
         tc_fence_before();
@@ -305,15 +320,14 @@ __global__ void __launch_bounds__(256, TcCfg<R>::MINB)
         {
             // row (l, n2): Y[k1] at columns k1 (real) and R + k1 (imaginary)
             float re[H], im[H];
-            tc_ld_half<R>(trow, c0, re, im);
+            tc_ld_part<R, H>(trow, c0, re, im);
             const float2* tw = reinterpret_cast<const float2*>(sm + C::OFF_TW) + rr * C::TWLD + c0;
             // ---- stage 2: A row (l, k1), column n2 (real) / R + n2 (imaginary) ----
 #pragma unroll
             for (int i = 0; i < H; ++i) {
                 const float2 u = cmulf(make_float2(re[i], im[i]), tw[i]);
-                const int m = l * R + c0 + i;
-                put_split1<R>(sm, a_off<R>(m, rr), u.x);
-                put_split1<R>(sm, a_off<R>(m, R + rr), u.y);
+                put_split1<R>(sm, base2 + step2(i), u.x);
+                put_split1<R>(sm, base2 + step2(i) + IM, u.y);
             }
         }
         fence_proxy_async_smem();
@@ -329,7 +343,7 @@ __global__ void __launch_bounds__(256, TcCfg<R>::MINB)
         {
             // row (l, k1): X[k1 + R k2] at columns k2 and R + k2
             float re[H], im[H];
-            tc_ld_half<R>(trow, c0, re, im);
+            tc_ld_part<R, H>(trow, c0, re, im);
             const int64_t line = tile * C::LINES + l;
             if (ok && line < nlines) {
                 float2* o = dst + line * L + rr + R * c0;
@@ -408,9 +422,9 @@ cudaError_t gen_tables(unsigned char (*tab)[TcCfg<R>::TAB_BYTES]) {
     return cudaGetLastError();
 }
 
-template <int R>
+template <int R, int TPR>
 cudaError_t launch_tc(const PassParams& p, int dir, int xconj, cudaStream_t st) {
-    using C = TcCfg<R>;
+    using C = TcCfg<R, TPR>;
     static std::mutex mu;
     static int grid_by_dev[64] = {0};
     int dev = 0;
@@ -422,17 +436,17 @@ cudaError_t launch_tc(const PassParams& p, int dir, int xconj, cudaStream_t st) 
         std::lock_guard<std::mutex> lk(mu);
         grid = grid_by_dev[dev];
         if (grid == 0) {
-            e = cudaFuncSetAttribute(k_tc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+            e = cudaFuncSetAttribute(k_tc<R, TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
             if (e != cudaSuccess) return e;
             // the whole unified L1 as shared memory: two (R = 32) CTAs an SM need it
-            e = cudaFuncSetAttribute(k_tc<R>, cudaFuncAttributePreferredSharedMemoryCarveout,
+            e = cudaFuncSetAttribute(k_tc<R, TPR>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared);
             if (e != cudaSuccess) return e;
             // resident CTAs an SM: shared memory (1 KB reserved a CTA), registers (a
             // warp's allocation rounded to 256), threads, and the SM's 512 tensor-memory
             // columns (2R a CTA); the occupancy query reports one CTA where two fit
             cudaFuncAttributes fa;
-            e = cudaFuncGetAttributes(&fa, k_tc<R>);
+            e = cudaFuncGetAttributes(&fa, k_tc<R, TPR>);
             if (e != cudaSuccess) return e;
             int nsm = 0, smem_sm = 0;
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -446,7 +460,7 @@ cudaError_t launch_tc(const PassParams& p, int dir, int xconj, cudaStream_t st) 
     const int64_t ntiles = (p.nlines + C::LINES - 1) / C::LINES;
     if (ntiles <= 0) return cudaSuccess;
     const int g = (int)std::min<int64_t>(grid, ntiles);
-    k_tc<R><<<g, C::NT, C::SMEM, st>>>(p, dir, xconj);
+    k_tc<R, TPR><<<g, C::NT, C::SMEM, st>>>(p, dir, xconj);
     return cudaGetLastError();
 }
 
@@ -488,8 +502,10 @@ cudaError_t tc_launch(const PassParams& p, int L, cudaStream_t st) {
     // conj(F(conj(a x))) = a F^-1 x: both sides conjugating is the inverse transform
     const int dir = lc && sc ? 1 : 0;
     const int xconj = dir ? 0 : (lc ? 1 : 0) | (sc ? 2 : 0);
-    if (L == 1024) return launch_tc<32>(p, dir, xconj, st);
-    if (L == 256) return launch_tc<16>(p, dir, xconj, st);
+    // threads a row: 4 for 1024-point lines (32 warps an SM: 83.8 us against 87.6 with
+    // 2 on 16384 lines), 2 for 256-point ones (70.8 us against 76.6 with 4 on 65536)
+    if (L == 1024) return launch_tc<32, 4>(p, dir, xconj, st);
+    if (L == 256) return launch_tc<16, 2>(p, dir, xconj, st);
     return cudaErrorInvalidValue;
 }
 
