@@ -103,6 +103,10 @@ extern "C" {
 #define RK_FLAG_BATCHABLE 2048 /* plan only passes the persistent batched kernel has tile bodies for
                                 (no plane pass, strided fused Bluestein lines of at most 1024
                                 points); rk_batch_create members */
+#define RK_FLAG_BLUE_PAIR 4096 /* 8192-point complex64 fused Bluestein lines on a two-CTA
+                                cluster a line (each CTA one half of the padded spectrum, one
+                                exchange through distributed shared memory) instead of one CTA;
+                                tuning (about 11% faster below 100 lines, slower from 500) */
 #define RK_FLAG_R16 1024      /* 8192-point complex64 fused Bluestein lines with 16 elements a
                                 thread on 512 threads instead of 32 on 256 (tuning) */
 #define RK_FLAG_NO_HALF 512   /* never run a real signal's last-axis transform as the half-length

@@ -50,6 +50,7 @@ FLAG_ANTIPERIODIC = 256
 FLAG_NO_HALF = 512
 FLAG_R16 = 1024
 FLAG_BATCHABLE = 2048
+FLAG_BLUE_PAIR = 4096  # fused 8192-point Bluestein lines on a two-CTA cluster a line (tuning)
 
 EXPORTED = (
     "rk_edge_init",

@@ -11,8 +11,10 @@ measured on the caller's own arguments and the fastest is kept:
   launch (``FLAG_PAIR``), or separate line passes (``FLAG_NO_PLANE``);
 * operand staging: persistent TMA-fed line passes or plain per-tile loads
   (``FLAG_NO_TMA``);
-* threads per transform and radix plan of 8192-point Bluestein lines: 32 elements a
-  thread on 256 threads, or 16 on 512 (``FLAG_R16``);
+* threads per transform and radix plan of 8192-point Bluestein lines: one CTA of 256
+  threads with 32 elements a thread (the default), 16 on 512 (``FLAG_R16``), or a
+  two-CTA cluster a line, each CTA one half of the padded spectrum
+  (``FLAG_BLUE_PAIR``);
 * Bluestein in one fused pass or as separate FFT passes (``FLAG_NO_BLUE1``);
 * a real signal's transform as the half-length FFT of sample pairs or at full length
   (``FLAG_NO_HALF``);
@@ -44,8 +46,8 @@ def candidates(comp, allow_split: bool = False) -> list[int]:
     blue = [p for p in passes if p["var"] & 15 == 1]
     if blue:
         out.append(N.FLAG_NO_BLUE1)
-        if any(p["L"] == 8192 and p["mode"] == "pos" for p in blue):
-            out.append(N.FLAG_R16)
+        if any(p["L"] == 8192 and p["mode"] == "pos" and p["var"] & 15 == 1 for p in blue):
+            out += [N.FLAG_R16, N.FLAG_BLUE_PAIR]
     if any(p["note"] == "half" for p in passes):
         out.append(N.FLAG_NO_HALF)
     if allow_split and any(p["kind"] == "line" and p["L"] == 1024 and p["mode"] == "pos" and p["var"] == 0

@@ -52,6 +52,8 @@ struct PlaneInfo {
 
 // lookup; returns false if the combination is not compiled
 bool line_info(int dbl, int L, int mode, int var, LineInfo* out);
+// fused Bluestein pass on a two-CTA cluster a line (variant 7, rk_blue2.cu); L = M/2
+bool blue2_info(int dbl, int L, LineInfo* out);
 bool plane_info(int dbl, int L1, int L2, int wide, PlaneInfo* out);
 
 // row + column passes of a plane in one persistent launch (rk_pair.cu)

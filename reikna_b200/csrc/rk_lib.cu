@@ -41,6 +41,7 @@ static thread_local std::string g_err;
 void set_error(const std::string& msg) { g_err = msg; }
 
 bool line_info(int dbl, int L, int mode, int var, LineInfo* out) {
+    if (var == 7) return mode == MODE_POS && blue2_info(dbl, L, out);
     return dbl ? line_info_f64(L, mode, var, out) : line_info_f32(L, mode, var, out);
 }
 
@@ -518,6 +519,15 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
                 // RK_FLAG_R16: 8192-point float32 lines on the 16-element plan with 512
                 // threads (variant bit 16) instead of 32 elements on 256 threads
                 if (!dbl && M == 8192 && I == 1 && (d.flags & RK_FLAG_R16)) p.var = 1 + 16;
+                // RK_FLAG_BLUE_PAIR: 8192-point float32 lines on a two-CTA cluster
+                // (variant 7, L = M/2 a CTA); not for the persistent batch kernel or
+                // user edge code
+                const bool pair2 = !dbl && M == 8192 && I == 1 && p.var == 1 && (d.flags & RK_FLAG_BLUE_PAIR) &&
+                                   !(d.flags & RK_FLAG_BATCHABLE) && !desc_has_user(d);
+                if (pair2) {
+                    p.L = (int)(M / 2);
+                    p.var = 7;
+                }
                 p.axis = ax;
                 p.O = O; p.C = 1; p.I = I;
                 p.ld.buf = cur; p.ld.ax_len = n; p.ld.cA = 0; p.ld.jB = 1;
@@ -525,7 +535,7 @@ static int plan_passes(const rk_fft_desc& d, Planned& P) {
                 const int out = last_axis ? SB_OUT : array_out(true);
                 p.st.buf = out; p.st.ax_len = n; p.st.cA = 0; p.st.jB = 1;
                 p.st.flags = SF_PRE_CONJ | SF_CHIRP; p.st.chirp_axis = ax;
-                p.note = "bluestein-fused";
+                p.note = pair2 ? "bluestein-pair" : "bluestein-fused";
                 P.passes.push_back(p);
                 cur = out;
             } else {
@@ -1173,7 +1183,7 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         r.dbl = dbl;
         r.L = ps.L;
         r.mode = ps.mode;
-        r.blue = (ps.var & 15) == 1;
+        r.blue = (ps.var & 15) == 1 || ps.var == 7;
         r.var = ps.var;
         r.axis = ps.axis;
         r.ld_buf = ps.ld.buf == SB_IN ? BUF_IN : ps.ld.buf == SB_OUT ? BUF_OUT : ps.ld.buf;
@@ -1266,6 +1276,15 @@ int rk_fft_plan_create(const rk_fft_desc* desc, rk_fft_plan** out) {
         }
         if (ps.st.chirp_axis >= 0) pp.st.chirp = blue_tabs[ps.st.chirp_axis].first;
         if (ps.blue_axis >= 0) pp.blue_k = blue_tabs[ps.blue_axis].second;
+        if (ps.var == 7) {
+            // W_M^n, n = 0 .. L, for the odd-bin CTA of the two-CTA Bluestein pass
+            void* wt = nullptr;
+            const int rc7 = alloc((int64_t)(ps.L + 1) * 8, &wt);
+            if (rc7) return fail(rc7);
+            k_gen_rpost<<<(unsigned)((ps.L + 256) / 256), 256>>>(ps.L, (float2*)wt, nullptr);
+            CK(cudaGetLastError());
+            pp.rtwid = wt;
+        }
         {
             const int lg = ilog2(std::max(ps.L, 1));
             const int lg2 = ilog2(std::max(ps.kind == PK_PLANE ? ps.L1 : ps.L, 1));
