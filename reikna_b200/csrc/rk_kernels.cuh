@@ -869,23 +869,35 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
                                                          [&](int i) { return pair_pos<L, RT, TPL>(tb, i, p.rodd); }, v);
         } else {
             __syncthreads();
+            // the lane-fastest read-back takes a warp's 32 / NL positions of NL lines
+            // at once: a line stride of L + 32 / NL (8-byte words; not the engine's
+            // L + L / 16, a multiple of 16 words, which put all NL lines of a position
+            // on one bank) spreads them over the banks; it fits the engine's buffer
+            // whenever 32 / NL <= L / 16
+            constexpr int D = NL >= 32 ? 1 : 32 / NL;
+            constexpr bool PAD = D <= L / 16;
+            auto ts = [&](int l, int pos) { return PAD ? l * (L + D) + pos : E::sidx(l, pos); };
 #pragma unroll
-            for (int i = 0; i < RT; ++i) sm[E::sidx(ln, pair_pos<L, RT, TPL>(tb, i, p.rodd))] = v[i];
+            for (int i = 0; i < RT; ++i) sm[ts(ln, pair_pos<L, RT, TPL>(tb, i, p.rodd))] = v[i];
             __syncthreads();
             const int lane = tid % NL;
             const int p0 = tid / NL;
             const int64_t sline = block * NL + lane;
             const LineAddr ls = line_addr(p.st, sline, p.C, p.I, sline < p.nlines);
 #pragma unroll
-            for (int q = 0; q < RT; ++q) v[q] = sm[E::sidx(lane, p0 + TPL * q)];
+            for (int q = 0; q < RT; ++q) v[q] = sm[ts(lane, p0 + TPL * q)];
             store_block<T, RT, STORE_FAST | STORE_FASTR>(p.st, p, ls, [&](int q) { return p0 + TPL * q; }, v);
         }
     } else if constexpr (VAR == 2) {
         static_assert(MODE == MODE_POS, "transposed store needs position mode");
+        // line stride L + 32 / NL for the lane-fastest read-back (as in variant 5)
+        constexpr int D = NL >= 32 ? 1 : 32 / NL;
+        constexpr bool PAD = D <= L / 16;
+        auto ts = [&](int l, int pos) { return PAD ? l * (L + D) + pos : E::sidx(l, pos); };
 #pragma unroll
         for (int z = 0; z < RT / RL; ++z)
 #pragma unroll
-            for (int m = 0; m < RL; ++m) sm[E::sidx(ln, E::out_pos(tb, z, m))] = v[z * RL + m];
+            for (int m = 0; m < RL; ++m) sm[ts(ln, E::out_pos(tb, z, m))] = v[z * RL + m];
         __syncthreads();
         // thread t stores lane t % NL, positions t / NL + TPL * q
         const int lane = tid % NL;
@@ -893,7 +905,7 @@ __device__ __forceinline__ void line_body(const PassParams& p, int64_t block, un
         const int64_t sline = block * NL + lane;
         const LineAddr la = line_addr(p.st, sline, p.C, p.I, sline < p.nlines);
 #pragma unroll
-        for (int q = 0; q < RT; ++q) v[q] = sm[E::sidx(lane, p0 + TPL * q)];
+        for (int q = 0; q < RT; ++q) v[q] = sm[ts(lane, p0 + TPL * q)];
         store_block<T, RT>(p.st, p, la, [&](int q) { return p0 + TPL * q; }, v);
     } else {
         const LineAddr la = line_addr(p.st, line, p.C, p.I, lok);
