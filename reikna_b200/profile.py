@@ -6,6 +6,8 @@ events around every pass (``rk_fft_profile``).
 
   python -m reikna_b200.profile --shape 256,256,256 [--axes 0,1,2] [--shift-scale]
       [--dtype complex64|complex128] [--flags N] [--steps 4] [--reps 200]
+  python -m reikna_b200.profile --spectrogram 4194304 [--nfft 1024] [--hop 256]
+      [--transposed] [--steps 4] [--reps 200]
 """
 
 from __future__ import annotations
@@ -17,7 +19,11 @@ import sys
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--shape", required=True, help="comma-separated array shape")
+    ap.add_argument("--shape", help="comma-separated array shape")
+    ap.add_argument("--spectrogram", type=int, default=0, help="signal length: profile the spectrogram instead")
+    ap.add_argument("--nfft", type=int, default=1024)
+    ap.add_argument("--hop", type=int, default=256)
+    ap.add_argument("--transposed", action="store_true", help="spectrogram stored bins by frames")
     ap.add_argument("--axes", default=None, help="comma-separated transformed axes (default: all)")
     ap.add_argument("--dtype", default="complex64", choices=["complex64", "complex128"])
     ap.add_argument("--shift-scale", action="store_true", help="fused output fftshift and 1/N")
@@ -31,6 +37,10 @@ def main(argv=None) -> int:
     from . import transformations as tr
     from .fft import FFT
 
+    if args.spectrogram:
+        return _spectrogram(args)
+    if not args.shape:
+        ap.error("--shape or --spectrogram is required")
     shape = tuple(int(v) for v in args.shape.split(","))
     axes = None if args.axes is None else tuple(int(v) for v in args.axes.split(","))
     dev = torch.device("cuda", 0)
@@ -49,7 +59,6 @@ def main(argv=None) -> int:
     for _ in range(args.steps):
         cc(None, y, x)
     torch.cuda.synchronize()
-    plan = cc._runner.plan
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.record()
     for _ in range(args.reps):
@@ -57,16 +66,52 @@ def main(argv=None) -> int:
     e.record()
     torch.cuda.synchronize()
     step_us = s.elapsed_time(e) / args.reps * 1e3
-    plan.profile(args.reps)
-    for _ in range(args.reps):
-        cc(None, y, x)
+    out = {"shape": list(shape), "axes": axes, "dtype": args.dtype, "flags": args.flags, "us_per_step": step_us,
+           "passes": _passes(cc, lambda: cc(None, y, x), args.reps)}
+    print(json.dumps(out))
+    return 0
+
+
+def _passes(cc, call, reps: int) -> list:
+    """Per-pass CUDA-event times of ``reps`` calls of a compiled FFT-based computation."""
+    import torch
+
+    plan = cc._runner.plan
+    plan.profile(reps)
+    for _ in range(reps):
+        call()
     torch.cuda.synchronize()
     ms, calls = plan.profile_read()
     plan.profile(0)
-    passes = plan.describe()["passes"]
-    out = {"shape": list(shape), "axes": axes, "dtype": args.dtype, "flags": args.flags, "us_per_step": step_us,
-           "passes": [{"note": p["note"], "L": p["L"], "mode": p["mode"], "var": p["var"],
-                       "us": m / max(1, calls) * 1e3} for p, m in zip(passes, ms)]}
+    return [{"note": p["note"], "L": p["L"], "mode": p["mode"], "var": p["var"], "us": m / max(1, calls) * 1e3}
+            for p, m in zip(plan.describe()["passes"], ms)]
+
+
+def _spectrogram(args) -> int:
+    import torch
+
+    from .spectrogram import frames, spectrogram
+
+    dev = torch.device("cuda", 0)
+    n = args.spectrogram
+    gen = torch.Generator(device=dev).manual_seed(1)
+    x = torch.randn(n, device=dev, dtype=torch.float32, generator=gen)
+    nf = frames(n, args.nfft, args.hop)
+    nb = args.nfft // 2 + 1
+    y = torch.empty((nb, nf) if args.transposed else (nf, nb), device=dev, dtype=torch.float32)
+    cc = spectrogram(n, args.nfft, args.hop, transposed=args.transposed).compile(dev)
+    for _ in range(args.steps):
+        cc(None, y, x)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(args.reps):
+        cc(None, y, x)
+    e.record()
+    torch.cuda.synchronize()
+    out = {"spectrogram": n, "nfft": args.nfft, "hop": args.hop, "transposed": args.transposed,
+           "us_per_step": s.elapsed_time(e) / args.reps * 1e3,
+           "passes": _passes(cc, lambda: cc(None, y, x), args.reps)}
     print(json.dumps(out))
     return 0
 
