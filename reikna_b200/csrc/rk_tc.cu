@@ -358,6 +358,9 @@ __global__ void __launch_bounds__(TcCfg<R, TPR>::NT, TcCfg<R, TPR>::MINB)
         }
         tc_fence_before();
     }
+    // after a timed-out wait the last committed products may still be running: wait for
+    // their commit once more (bounded) before the tensor memory they write is freed
+    if (!ok) mbar_wait(bar, phase ^ 1, p.status);
     // all tensor-memory reads are done (or abandoned after a timed-out wait)
     tc_fence_before();
     __syncthreads();
