@@ -8,7 +8,13 @@ namespace rk {
 
 template <typename T, int L, int MODE> struct TmaCfg {
     using Cfg = LineCfg<T, L, MODE>;
-    static constexpr int NL = Cfg::NL, NT = Cfg::NT, ESZ = Cfg::ESZ;
+    static constexpr int ESZ = Cfg::ESZ;
+    // lane mode: lines a CTA halved (down to one 128-byte segment of lines) while a tile
+    // exceeds 32 KB, so that its two buffers leave room for more than one CTA an SM
+    // (complex128 128-point lines: 32 -> 16 lines, 133 -> 66 KB)
+    static constexpr int NL_HALF = Cfg::NL / 2 >= Vec<T>::N && Cfg::NL * L * ESZ > 32768 ? Cfg::NL / 2 : Cfg::NL;
+    static constexpr int NL = MODE == MODE_LANE ? NL_HALF : Cfg::NL;
+    static constexpr int NT = NL * Cfg::TPL;
     static constexpr int TILE = NL * L;                                           // elements copied
     static constexpr int BUF = MODE == MODE_POS ? NL * Cfg::LS : NL * L;          // elements per buffer
     static constexpr size_t SMEM0 = 2 * (size_t)BUF * ESZ + 64;                    // + mbarriers
@@ -20,10 +26,10 @@ template <typename T, int L, int MODE> struct TmaCfg {
 };
 
 template <typename T, int L, int MODE>
-__global__ void __launch_bounds__(LineCfg<T, L, MODE>::NT) k_line_tma(const __grid_constant__ PassParams p) {
+__global__ void __launch_bounds__(TmaCfg<T, L, MODE>::NT) k_line_tma(const __grid_constant__ PassParams p) {
     using V = cplx<T>;
-    using E = Engine<T, L, MODE>;
     using C = TmaCfg<T, L, MODE>;
+    using E = Engine<T, L, MODE, 0, C::NL>;
     constexpr int RT = E::RT, TPL = E::TPL, NL = E::NL, R0 = E::R0, RL = E::RL;
     extern __shared__ __align__(128) unsigned char rk_smem[];
     V* buf0 = reinterpret_cast<V*>(rk_smem);
