@@ -9,10 +9,11 @@ namespace rk {
 template <typename T, int L, int MODE> struct TmaCfg {
     using Cfg = LineCfg<T, L, MODE>;
     static constexpr int ESZ = Cfg::ESZ;
-    // lane mode: lines a CTA halved (down to one 128-byte segment of lines) while a tile
-    // exceeds 32 KB, so that its two buffers leave room for more than one CTA an SM
-    // (complex128 128-point lines: 32 -> 16 lines, 133 -> 66 KB)
-    static constexpr int NL_HALF = Cfg::NL / 2 >= Vec<T>::N && Cfg::NL * L * ESZ > 32768 ? Cfg::NL / 2 : Cfg::NL;
+    // lane mode: lines a CTA halved (down to half a 128-byte segment of lines) where a
+    // tile exceeds 32 KB, so that its two buffers leave room for more than one CTA an SM
+    // (complex128 128-point lines: 32 -> 16 lines, 133 -> 66 KB; complex64 512-point
+    // lines: 16 -> 8, 64-byte rows)
+    static constexpr int NL_HALF = Cfg::NL / 2 >= Vec<T>::N / 2 && Cfg::NL * L * ESZ > 32768 ? Cfg::NL / 2 : Cfg::NL;
     static constexpr int NL = MODE == MODE_LANE ? NL_HALF : Cfg::NL;
     static constexpr int NT = NL * Cfg::TPL;
     static constexpr int TILE = NL * L;                                           // elements copied
