@@ -27,9 +27,10 @@
 // transform uses the conjugate tables instead of conjugating data.
 //
 // The grid is persistent: two CTAs of 512 threads an SM (R = 32, four threads a row)
-// or four of 256 (R = 16, two a row); a thread prefetches the next tile's input into registers while the current tile is
-// on the tensor cores.  Tensor memory (2R columns) is allocated once a CTA and freed
-// before exit, also after a timed-out wait; every wait is clock-bounded.
+// or four of 256 (R = 16, two a row); a thread prefetches the next tile's input into
+// registers while the current tile is on the tensor cores.  Tensor memory (2R columns)
+// is allocated once a CTA and freed before exit, also after a timed-out wait (after a
+// second bounded wait for the products in flight); every wait is clock-bounded.
 #include <cuda_runtime.h>
 
 #include <algorithm>
